@@ -1,0 +1,402 @@
+"""Benchmark of the B200 SCALE-DG advection RHS (one JSON line on rank 0).
+
+Workload (default): plain FP64 DG advection at 32^3 elements, p = 7
+(16,777,216 DOF), the OPT1-equivalent kernels in FMA form ("GPU"), constant
+velocity (1, 0.5, 0.25), the seeded Gaussian + Fourier initial condition,
+dt = 0.1 h / (p+1)^2.  A bench step is one SSP-RK3 time step (three
+right-hand-side evaluations fused with their stage updates).  Metric:
+DOF-updates per second per RHS evaluation = Ne*Np*3*K / time.
+
+  value  device-resident state, K steps timed with CUDA events on the
+         library's stream (inputs of 537 MB > 126 MB L2, so no L2 flush).
+  e2e    the same steps through the C ABI with host buffers: each step
+         uploads the state q from pinned host memory (sdg_set_field), runs
+         the step (sdg_rk3_steps) and reads q back (sdg_get_field).
+  e2e_cal_tend  the drop-in advect3d_eq_cal_tend call (sdg_cal_tend):
+         q,u,v,w(Np,NeA) in, dqdt(Np,Ne) out per RHS evaluation.
+  roofline  the fused stage kernel: algorithmic bytes (40/48/48 B per DOF
+         for stages 1/2/3) over its CUDA-event duration, against the
+         measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (restated reference OPT1 path) on the host
+         cores, a bounded sample of the same workload (rank 0, N = 1).
+
+--impl reference runs the reference's CPU path (the oracle restatement; the
+Fortran reference cannot be compiled in this image) on all host threads, a
+bounded number of RK3 steps of the same workload, and prints its own line.
+
+Multi-GPU (torchrun, N > 1): independent replicas, one per GPU (the path
+has no data exchange on one mesh per device), weak scaling, time = max over
+ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "scale-dg-kernel-extraction_b200"))
+
+WORKLOADS = {
+    # name: (NeX, NeY, NeZ, p, flags-name, vel)
+    "fp64_32c_p7": (32, 32, 32, 7, "GPU", (1.0, 0.5, 0.25)),
+    "fp64_8c_p3": (8, 8, 8, 3, "GPU", (1.0, 0.5, 0.25)),
+    "mixed_32c_p7": (32, 32, 32, 7, "MIXED", "divfree"),
+    "mixed_16c_p15": (16, 16, 16, 15, "MIXED", "divfree"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="fp64_32c_p7", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="budget of the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(workload):
+    """Per-launch DRAM bytes of the fused stage kernel from the committed ncu
+    summary (profiles/<kernel>_<workload>.json), or None."""
+    path = os.path.join(REPO, "profiles", f"tend_stage_{workload}.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def build_problem(workload, sdg):
+    NeX, NeY, NeZ, p, kind, vel = WORKLOADS[workload]
+    flags = {"GPU": 0, "OPT1": sdg.FLAG_EXACT, "MIXED": sdg.FLAG_MIXED}[kind]
+    ops = sdg.read_operators(p)
+    mesh = sdg.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
+    if vel == "divfree":
+        q, u, v, w = sdg.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=1)
+    else:
+        q, u, v, w = sdg.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=0, vel=vel)
+    h = 1.0 / max(NeX, NeY, NeZ)
+    dt = 0.1 * h / (p + 1) ** 2
+    return ops, mesh, flags, (q, u, v, w), dt
+
+
+def stage_bytes_per_dof(mixed):
+    # Algorithmic bytes per DOF of stages 1..3: reads q (+ q0) + u, v, w,
+    # writes q_new.  FP64: 8-byte everything; mixed: FP32 velocity and
+    # stage intermediates, FP64 q0 and final q.
+    if mixed:
+        return [8 + 12 + 4, 4 + 12 + 8 + 4, 4 + 12 + 8 + 8]
+    return [8 + 24 + 8, 8 + 24 + 8 + 8, 8 + 24 + 8 + 8]
+
+
+def cpu_baseline(workload, seconds):
+    """The CPU oracle (restated reference OPT1 path) on all host threads:
+    repeated tendency evaluations of the same workload for ~`seconds`."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import orc
+    NeX, NeY, NeZ, p, kind, vel = WORKLOADS[workload]
+    ops = orc.read_operators(p)
+    mesh = orc.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
+    if vel == "divfree":
+        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=1)
+    else:
+        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=0, vel=vel)
+    orc.cal_tend(orc.OPT1, q, u, v, w, ops, mesh)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        orc.cal_tend(orc.OPT1, q, u, v, w, ops, mesh)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 200:
+            break
+    dof = mesh.Ne * mesh.Np
+    return {"value": dof * n / el, "unit": "DOF-updates/s per RHS eval",
+            "cores": orc.num_threads(), "kind": "port",
+            "sample": f"{n} tendency evaluations (OPT1 order) of the {workload} "
+                      f"workload, {el:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (oracle restatement) on all
+    host threads, RK3 steps of the same workload; rank 0 only."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import orc
+    NeX, NeY, NeZ, p, kind, vel = WORKLOADS[args.workload]
+    ops = orc.read_operators(p)
+    mesh = orc.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
+    if vel == "divfree":
+        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=1)
+    else:
+        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=0, vel=vel)
+    dt = 0.1 / max(NeX, NeY, NeZ) / (p + 1) ** 2
+    # Bounded sample: at most ~90 s of timed CPU work.
+    t0 = time.perf_counter()
+    orc.run_rk3(orc.OPT1, q, u, v, w, ops, mesh, dt, max(1, min(args.warmup, 3)))
+    t_step = (time.perf_counter() - t0) / max(1, min(args.warmup, 3))
+    k = max(1, min(args.steps, int(90.0 / max(t_step, 1e-6))))
+    _, times = orc.run_rk3(orc.OPT1, q, u, v, w, ops, mesh, dt, k)
+    dof = mesh.Ne * mesh.Np
+    val = dof * 3 * k / times[0]
+    line = {
+        "impl": "reference", "metric": "DOF-updates/s per RHS eval", "value": val,
+        "unit": "DOF-updates/s per RHS eval", "n_gpus": args.gpus, "steps": k,
+        "warmup": args.warmup, "ms_per_step": 1e3 * times[0] / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "mesh": [NeX, NeY, NeZ], "p": p,
+                   "dof": dof, "evaltype": "OPT1", "nstep_timed": k},
+        "cpu_baseline": {"value": val, "unit": "DOF-updates/s per RHS eval",
+                         "cores": orc.num_threads(), "kind": "port",
+                         "sample": f"{k} of {args.steps} requested SSP-RK3 steps of the "
+                                   f"{args.workload} workload (restated reference OPT1 "
+                                   "path; the Fortran reference cannot be compiled here)"},
+        "e2e": {"value": val, "unit": "DOF-updates/s per RHS eval",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    import sdg_b200 as sdg
+
+    ops, mesh, flags, (q, u, v, w), dt = build_problem(args.workload, sdg)
+    mixed = bool(flags & sdg.FLAG_MIXED)
+    H = sdg.Handle(ops, mesh, flags)
+    H.set_state(q, u, v, w)
+    stream = torch.cuda.ExternalStream(H.stream())
+    dof = mesh.Ne * mesh.Np
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up ----
+    H.rk3_steps(dt, args.warmup)
+    H.synchronize()
+
+    # ---- timed region: K RK3 steps, device-resident ----
+    l0 = H.launch_count()
+    gpu_idx = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            gpu_idx = int(vis.split(",")[local])
+        except ValueError:
+            pass
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_idx) as clk:
+        barrier()
+        ev0.record(stream)
+        H.rk3_steps(dt, args.steps)
+        ev1.record(stream)
+        H.synchronize()
+        barrier()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    launches = H.launch_count() - l0
+    t_max = max_over_ranks(t)
+    value = world * dof * 3 * args.steps / t_max
+
+    # ---- per-stage kernel durations (roofline) ----
+    reps = 30
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(reps)]
+    for r in range(reps):
+        evs[r][0].record(stream)
+        for s in (1, 2, 3):
+            H.rk3_stage(s, dt)
+            evs[r][s].record(stream)
+    H.synchronize()
+    stage_ms = [statistics.median(evs[r][s - 1].elapsed_time(evs[r][s]) for r in range(reps))
+                for s in (1, 2, 3)]
+    bpd = stage_bytes_per_dof(mixed)
+    alg_bytes = [b * dof for b in bpd]
+    achieved = sum(alg_bytes) / (sum(stage_ms) * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic(args.workload)
+
+    # ---- e2e: RK3 steps through the C ABI with host buffers ----
+    n_e2e = max(3, min(20, args.steps // 50))
+    NE = mesh.Np * mesh.Ne
+    q_pin = torch.empty(NE, dtype=torch.float64, pin_memory=True)
+    q_pin.numpy()[:] = q.reshape(-1, order="F")[:NE]
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        H.set_field(sdg.FIELD_Q, q_pin.numpy())
+        H.rk3_steps(dt, 1)
+        out = H.get_field(sdg.FIELD_Q)
+        q_pin.numpy()[:] = out.reshape(-1, order="F")
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * dof * 3 * n_e2e / t_e2e
+
+    # ---- e2e of the drop-in tendency call (FP64 handles only) ----
+    e2e_ct = None
+    if not mixed:
+        NA = mesh.Np * mesh.NeA
+        pins = [torch.empty(NA, dtype=torch.float64, pin_memory=True) for _ in range(5)]
+        for pt, a in zip(pins, (q, u, v, w)):
+            pt.numpy()[:] = a.reshape(-1, order="F")
+        Hc = sdg.Handle(ops, mesh, flags)
+        arrs = [pt.numpy().reshape(mesh.Np, mesh.NeA, order="F") for pt in pins]
+        Hc.cal_tend(*arrs[:4], dqdt=arrs[4])
+        n_ct = 5
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(n_ct):
+            Hc.cal_tend(*arrs[:4], dqdt=arrs[4])
+        t_ct = max_over_ranks(time.perf_counter() - t0)
+        e2e_ct = {"value": world * dof * n_ct / t_ct, "unit": "DOF-updates/s per RHS eval",
+                  "h2d_bytes_per_step": 4 * NA * 8, "d2h_bytes_per_step": NE * 8}
+        Hc.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.workload, args.cpu_seconds)
+
+    if rank == 0:
+        NeX, NeY, NeZ, p, kind, vel = WORKLOADS[args.workload]
+        line = {
+            "metric": "DOF-updates/s per RHS eval", "value": value,
+            "unit": "DOF-updates/s per RHS eval", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "mesh": [NeX, NeY, NeZ], "p": p,
+                       "dof_per_gpu": dof, "evaltype": kind,
+                       "rhs_evals_per_step": 3, "dt": dt,
+                       "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": traffic,
+                         "kernel": "tend_kernel (fused flux+volume+lift+RK stage)",
+                         "stage_ms": stage_ms,
+                         "alg_bytes_per_dof": bpd},
+            "e2e": {"value": e2e, "unit": "DOF-updates/s per RHS eval",
+                    "h2d_bytes_per_step": NE * 8, "d2h_bytes_per_step": NE * 8,
+                    "api": "sdg_set_field + sdg_rk3_steps + sdg_get_field per step"},
+            "e2e_cal_tend": e2e_ct,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    H.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

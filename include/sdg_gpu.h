@@ -1,0 +1,203 @@
+/*
+ * sdg_gpu.h - C ABI of the B200 (sm_100a) SCALE-DG 3D DG advection library.
+ *
+ * The library replaces, at whole-mesh granularity, the hot path of
+ * seiya/scale-dg-kernel-extraction:
+ *
+ *   advect3d_eq_cal_tend      mod_advect3d_eq.f90:41-85   (flux + dqdt)
+ *   update_halo               mod_mesh.f90:209-221
+ *   SSP-RK3 stage update      main.f90:51-80, mod_common.f90:28-30
+ *
+ * and mirrors the host-side set-up the Fortran driver performs
+ * (element_init mod_mesh.f90:226-327, mesh_setup mod_mesh.f90:74-193) so a
+ * host program in any language can drive it.  Every symbol is extern "C"
+ * and Fortran bind(C)-compatible: scalars are passed by value (int32 or
+ * double), arrays as plain pointers in the reference's Fortran layout
+ * (column-major; VMapM, VMapP and halo_src_map hold 1-based indices), and
+ * every call returns an int status (SDG_OK = 0).  sdg_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Ownership: host arrays passed in are only read (or written, for outputs)
+ * during the call and stay owned by the caller.  Device buffers belong to
+ * the handle.  Threading: one host thread at a time per handle; each handle
+ * owns one CUDA stream; separate handles are independent.
+ *
+ * There is no CPU fallback: without a usable CUDA device, sdg_init fails
+ * with SDG_ERR_CUDA.
+ */
+#ifndef SDG_GPU_H
+#define SDG_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define SDG_OK 0
+#define SDG_ERR_ARG 1     /* invalid argument or size                    */
+#define SDG_ERR_CUDA 2    /* CUDA runtime error, or no device            */
+#define SDG_ERR_IO 3      /* operator file missing or malformed          */
+#define SDG_ERR_MESH 4    /* mesh tables not in the supported form       */
+#define SDG_ERR_STATE 5   /* call out of order (e.g. no state uploaded)  */
+
+/* sdg_init flags. */
+#define SDG_FLAG_EXACT 1          /* no FMA: every product and sum rounded
+                                     separately in the reference's order,
+                                     bit-for-bit the x86-64 reference      */
+#define SDG_FLAG_ORDER_GENERAL 2  /* GENERAL summation order (mod_dg_optr_
+                                     kernel.f90:221-257) instead of OPT1's
+                                     three partial sums for p > 7 (erb:242) */
+#define SDG_FLAG_MIXED 4          /* resident RK path in mixed precision:
+                                     FP32 velocity, tendency and stage
+                                     intermediates, FP64 RK accumulation   */
+
+/* Fields for sdg_set_field / sdg_get_field. */
+#define SDG_FIELD_Q 0
+#define SDG_FIELD_U 1
+#define SDG_FIELD_V 2
+#define SDG_FIELD_W 3
+
+typedef struct sdg_handle sdg_handle;
+
+/* Copies the last error message of this thread into buf (NUL-terminated,
+ * truncated to buflen); returns the message length. */
+int sdg_last_error(char* buf, int buflen);
+
+/* Library version string "major.minor.patch". */
+const char* sdg_version(void);
+
+/* ---------------------------------------------------------------------
+ * Host-side set-up (mirrors of the reference's Fortran set-up routines)
+ * --------------------------------------------------------------------- */
+
+/* element_init operator read (mod_mesh.f90:253-263): reads
+ * <dir>/p<p>.dat into x1D(Nq), D1D(Nq,Nq), Lift_mat(Nq,Nq,Nq,6).
+ * p must be 1..15.  SDG_ERR_IO on a missing or short file. */
+int sdg_read_operators(const char* dir, int p, double* x1D, double* D1D,
+                       double* Lift_mat);
+
+/* Mesh sizes of mesh_setup (mod_mesh.f90:96-100):
+ * sizes[0..5] = Ne, Nhalo, NeA, NhaloNode, Np, NfpTot.  Fails when
+ * Np*NeA would overflow the int32 index space of VMapM/VMapP. */
+int sdg_mesh_sizes(int NeX, int NeY, int NeZ, int p, int* sizes);
+
+/* Fmask(Nfp,6) of element_init (mod_mesh.f90:278-324), 1-based. */
+int sdg_fmask(int p, int* Fmask);
+
+/* mesh_setup (mod_mesh.f90:74-193) for the periodic box
+ * [0,domx]x[0,domy]x[0,domz]: VMapM, VMapP (NfpTot,Ne), halo_src_map
+ * (NhaloNode), normal_fn (NfpTot,Ne,3), Escale (Np,Ne,3), Fscale (NfpTot,Ne)
+ * and pos_en (Np,Ne,3), bit-identical to the reference's tables. */
+int sdg_mesh_setup(int NeX, int NeY, int NeZ, int p, double domx, double domy,
+                   double domz, const double* x1D, int* VMapM, int* VMapP,
+                   int* halo_src_map, double* normal_fn, double* Escale,
+                   double* Fscale, double* pos_en);
+
+/* update_halo (mod_mesh.f90:209-221) on a host array f(Np*NeA). */
+int sdg_update_halo_host(double* f, int Np, int Ne, int NhaloNode,
+                         const int* halo_src_map);
+
+/* Initial fields (main.f90:146-157 and the seeded workloads):
+ *   ic_kind 0: q = sin(2 pi x) sin(2 pi y) sin(2 pi z)   (main.f90:149-151)
+ *   ic_kind 1: Gaussian bump (sigma 0.1, cube centre) + 8 Fourier modes
+ *              (integer wavenumbers 1..4 per axis, amplitude N(0,0.01),
+ *              phase U[0,2 pi)) from a splitmix64 stream seeded by `seed`
+ *   vel_kind 0: constant (vx,vy,vz);  1: (sin 2 pi y, sin 2 pi z, sin 2 pi x)
+ * Writes q,u,v,w(:,1:Ne); halos are left to update_halo. */
+int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
+                    double vx, double vy, double vz, const double* pos_en,
+                    int Np, int Ne, double* q, double* u, double* v,
+                    double* w);
+
+/* A constant velocity drawn from U[-1,1]^3 by a splitmix64 stream. */
+int sdg_random_velocity(unsigned long long seed, double* vel3);
+
+/* ---------------------------------------------------------------------
+ * Handle: operators and mesh resident on the GPU
+ * --------------------------------------------------------------------- */
+
+/* Uploads the operators and mesh tables that advect3d_eq_cal_tend receives
+ * (mod_advect3d_eq.f90:41-65) plus halo_src_map (mod_mesh.f90:68), once.
+ * The verbatim tables are validated and compressed on the host: per-element
+ * Escale, per-face Fscale, axis-aligned normals and a per-face neighbour
+ * table equivalent node-for-node to VMapM/VMapP.  Tables that do not have
+ * that structure are rejected with SDG_ERR_MESH.  Replaces the selection
+ * of dg_optr_kernel_setup (mod_dg_optr_kernel.f90:45-58) for the "GPU"
+ * evaluation type; flags pick the arithmetic (SDG_FLAG_*). */
+int sdg_init(sdg_handle** h, int Nq, int Np, int NfpTot, int Ne, int NeA,
+             int NhaloNode, const double* D1D, const double* Lift_mat,
+             const int* VMapM, const int* VMapP, const int* halo_src_map,
+             const double* normal_fn, const double* Escale,
+             const double* Fscale, int flags);
+
+/* Releases the handle and its device memory. */
+int sdg_finalize(sdg_handle* h);
+
+/* Drop-in for advect3d_eq_cal_tend (mod_advect3d_eq.f90:41-85) on host
+ * arrays q,u,v,w(Np,NeA) (halo filled by the caller, as the reference
+ * reads it through VMapP) -> dqdt(Np,NeA), of which (:,1:Ne) is written.
+ * Copies in, runs the fused kernel, copies out; synchronous. */
+int sdg_cal_tend(sdg_handle* h, double* dqdt, const double* q,
+                 const double* u, const double* v, const double* w);
+
+/* The same on device arrays, asynchronously on `stream` (a cudaStream_t;
+ * NULL = the handle's stream). */
+int sdg_cal_tend_dev(sdg_handle* h, double* dqdt, const double* q,
+                     const double* u, const double* v, const double* w,
+                     void* stream);
+
+/* update_halo (mod_mesh.f90:209-221) on a device array f(Np*NeA). */
+int sdg_update_halo_dev(sdg_handle* h, double* f, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Resident RK3 path (main.f90:51-80 with the state kept in HBM)
+ * --------------------------------------------------------------------- */
+
+/* Uploads field `which` (SDG_FIELD_*) from a host array (Np,NeA) or
+ * (Np,Ne); only (:,1:Ne) is read, halos are rebuilt on the device. */
+int sdg_set_field(sdg_handle* h, int which, const double* host);
+
+/* Downloads the current state q(:,1:Ne) (FP64) into host (Np,Ne). */
+int sdg_get_field(sdg_handle* h, int which, double* host);
+
+/* Advances nsteps SSP-RK3 steps of size dt: each stage fuses the halo read,
+ * the tendency and the stage update in one kernel; steps replay a CUDA
+ * graph.  Asynchronous on the handle's stream. */
+int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps);
+
+/* min/max of q(:,1:Ne) (main.f90:76-79); synchronises the handle. */
+int sdg_minmax(sdg_handle* h, double* qmin, double* qmax);
+
+/* FP64 global diagnostics with the tensor LGL weights w(Nq) and the element
+ * Jacobian jac (= dx*dy*dz/8): mass = sum W*jac*q, l2 = sqrt(sum W*jac*q^2).
+ * Synchronises the handle. */
+int sdg_diagnostics(sdg_handle* h, const double* lgl_w, double jac,
+                    double* mass, double* l2);
+
+/* Enqueues stage `stage` (1..3) of one SSP-RK3 step (main.f90:58-74) on the
+ * handle's stream without a graph: stage 1 reads q0 and writes q1, stage 2
+ * reads q1 and q0 and writes q2, stage 3 reads q2 and q0 and overwrites q0.
+ * For timing and profiling single stage kernels. */
+int sdg_rk3_stage(sdg_handle* h, int stage, double dt);
+
+/* The handle's CUDA stream (a cudaStream_t) for event timing by callers. */
+int sdg_get_stream(sdg_handle* h, void** stream);
+
+/* Waits for all work queued on the handle's stream. */
+int sdg_synchronize(sdg_handle* h);
+
+/* Device pointer of a resident field (SDG_FIELD_Q gives the FP64 state). */
+int sdg_field_dev_ptr(sdg_handle* h, int which, void** ptr);
+
+/* Accumulated device time in seconds: t[0] = tendency/stage kernels of
+ * sdg_cal_tend*, t[1] = sdg_rk3_steps, t[2] = halo updates, t[3] = copies
+ * of sdg_cal_tend (host<->device). */
+int sdg_timers(sdg_handle* h, double* t4);
+
+/* Number of fused-kernel launches issued so far by the handle. */
+long long sdg_launch_count(sdg_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,767 @@
+// GPU core of the SCALE-DG advection library: the handle, validation and
+// compression of the reference's mesh tables, the resident SSP-RK3 path and
+// the small auxiliary kernels (halo gather, precision conversion, reductions).
+// The fused tendency kernel itself lives in sdg_tend.cuh and is instantiated
+// per polynomial order by sdg_tend_inst.cu.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "sdg_gpu.h"
+#include "sdg_internal.h"
+#include "sdg_launch.h"
+
+namespace sdg {
+namespace {
+
+#define SDG_CUDA(call)                                                     \
+  do {                                                                     \
+    cudaError_t err_ = (call);                                             \
+    if (err_ != cudaSuccess)                                               \
+      return fail(SDG_ERR_CUDA, "%s failed: %s", #call,                    \
+                  cudaGetErrorString(err_));                               \
+  } while (0)
+
+int launch_tend(const LaunchSpec& s) {
+  typedef int (*Fn)(const LaunchSpec&);
+  static const Fn table[17] = {nullptr,          nullptr,          launch_tend_nq2,
+                               launch_tend_nq3,  launch_tend_nq4,  launch_tend_nq5,
+                               launch_tend_nq6,  launch_tend_nq7,  launch_tend_nq8,
+                               launch_tend_nq9,  launch_tend_nq10, launch_tend_nq11,
+                               launch_tend_nq12, launch_tend_nq13, launch_tend_nq14,
+                               launch_tend_nq15, launch_tend_nq16};
+  if (s.nq < 2 || s.nq > 16) return fail(SDG_ERR_ARG, "Nq %d outside 2..16", s.nq);
+  const int rc = table[s.nq](s);
+  if (rc != 0)
+    return fail(SDG_ERR_CUDA, "fused tendency launch (Nq=%d) failed: %s", s.nq,
+                cudaGetErrorString(static_cast<cudaError_t>(rc)));
+  return SDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Auxiliary kernels
+// ---------------------------------------------------------------------------
+
+// f(Np*Ne + b) = f(src(b)), src 0-based (update_halo, mod_mesh.f90:216-218).
+template <typename T>
+__global__ void halo_kernel(T* __restrict__ f, const int* __restrict__ src,
+                            long base, int n) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n;
+       b += gridDim.x * blockDim.x)
+    f[base + b] = f[src[b]];
+}
+
+__global__ void to_f32_kernel(float* __restrict__ out,
+                              const double* __restrict__ in, long n) {
+  for (long x = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; x < n;
+       x += static_cast<long>(gridDim.x) * blockDim.x)
+    out[x] = static_cast<float>(in[x]);
+}
+
+constexpr int kRedThreads = 256;
+
+// Block-level reduction of NV values per thread; the last block to finish
+// folds the per-block partials (in block order, so the result is
+// deterministic) and resets the arrival counter.
+template <int NV, typename Op>
+__device__ void reduce_finish(double (&v)[NV], Op op, double* partials,
+                              unsigned int* counter, double* result) {
+  __shared__ double sh[NV][kRedThreads / 32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double x = v[i];
+    for (int o = 16; o > 0; o >>= 1) x = op(i, x, __shfl_down_sync(0xffffffffu, x, o));
+    if (lane == 0) sh[i][wid] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double x = sh[i][0];
+      for (int w = 1; w < kRedThreads / 32; ++w) x = op(i, x, sh[i][w]);
+      partials[NV * blockIdx.x + i] = x;
+    }
+    __threadfence();
+    const unsigned int done = atomicAdd(counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double x = partials[i];
+      for (unsigned int bk = 1; bk < gridDim.x; ++bk)
+        x = op(i, x, partials[NV * bk + i]);
+      result[i] = x;
+    }
+    *counter = 0u;
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads)
+    minmax_kernel(const double* __restrict__ q, long n, double* partials,
+                  unsigned int* counter, double* result) {
+  double v[2] = {INFINITY, -INFINITY};
+  for (long x = blockIdx.x * static_cast<long>(kRedThreads) + threadIdx.x; x < n;
+       x += static_cast<long>(gridDim.x) * kRedThreads) {
+    const double y = q[x];
+    v[0] = fmin(v[0], y);
+    v[1] = fmax(v[1], y);
+  }
+  reduce_finish<2>(v, [](int i, double a, double b) { return i == 0 ? fmin(a, b) : fmax(a, b); },
+                   partials, counter, result);
+}
+
+// mass = sum W(n) jac q, sumsq = sum W(n) jac q^2 with W(n) = w_i w_j w_k.
+__global__ void __launch_bounds__(kRedThreads)
+    moments_kernel(const double* __restrict__ q, const double* __restrict__ wn,
+                   int Np, long n, double jac, double* partials,
+                   unsigned int* counter, double* result) {
+  double v[2] = {0.0, 0.0};
+  for (long x = blockIdx.x * static_cast<long>(kRedThreads) + threadIdx.x; x < n;
+       x += static_cast<long>(gridDim.x) * kRedThreads) {
+    const double y = q[x];
+    const double wj = wn[x % Np] * jac;
+    v[0] += wj * y;
+    v[1] += wj * y * y;
+  }
+  reduce_finish<2>(v, [](int, double a, double b) { return a + b; }, partials,
+                   counter, result);
+}
+
+template <typename T>
+T* dev_alloc(size_t n, int* rc) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    *rc = fail(SDG_ERR_CUDA, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
+               cudaGetErrorString(e));
+    return nullptr;
+  }
+  return static_cast<T*>(p);
+}
+
+}  // namespace
+}  // namespace sdg
+
+using namespace sdg;
+
+struct sdg_handle {
+  int dev = 0;
+  int Nq = 0, Np = 0, NfpTot = 0, Ne = 0, NeA = 0, NhaloNode = 0;
+  int flags = 0;
+  bool direct_ok = false;
+  cudaStream_t stream = nullptr;
+  std::vector<double> D;  // row-major D(i,l)
+
+  // Compressed tables (device).
+  double* lift64 = nullptr;
+  float* lift32 = nullptr;
+  int* pb_halo = nullptr;
+  int* pb_direct = nullptr;
+  double* esc64 = nullptr;
+  float* esc32 = nullptr;
+  double* fsc64 = nullptr;
+  float* fsc32 = nullptr;
+  int* hsrc = nullptr;  // halo_src_map, 0-based
+
+  // sdg_cal_tend staging (lazy).
+  double* io[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+
+  // Resident state (lazy): FP64 Q0 always; stage buffers FP64 or FP32.
+  double* q0 = nullptr;
+  void* qa = nullptr;
+  void* qb = nullptr;
+  void* vel[3] = {nullptr, nullptr, nullptr};
+  double* vel64[3] = {nullptr, nullptr, nullptr};  // FP64 upload staging
+  bool have_vel[3] = {false, false, false};
+  bool have_q = false;
+
+  // Reductions.
+  double* red_partials = nullptr;
+  unsigned int* red_counter = nullptr;
+  double* red_result = nullptr;
+  double* lgl_wn = nullptr;
+  int red_blocks = 0;
+
+  // Step graph.
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = 0.0;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool rk_pending = false;   // ev0/ev1 bracket an unaccounted rk3 batch
+  double t_tend = 0, t_rk = 0, t_halo = 0, t_copy = 0;
+  long long launches = 0;
+};
+
+namespace {
+
+void free_handle(sdg_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  void* ptrs[] = {h->lift64, h->lift32, h->pb_halo, h->pb_direct, h->esc64,
+                  h->esc32,  h->fsc64,  h->fsc32,   h->hsrc,      h->io[0],
+                  h->io[1],  h->io[2],  h->io[3],   h->io[4],     h->q0,
+                  h->qa,     h->qb,     h->vel[0],  h->vel[1],    h->vel[2],
+                  h->vel64[0], h->vel64[1], h->vel64[2], h->red_partials,
+                  h->red_counter, h->red_result, h->lgl_wn};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+bool mixed(const sdg_handle* h) { return (h->flags & SDG_FLAG_MIXED) != 0; }
+
+LaunchSpec base_spec(const sdg_handle* h, bool f32) {
+  LaunchSpec s;
+  std::memset(&s, 0, sizeof(s));
+  s.nq = h->Nq;
+  s.exact = (h->flags & SDG_FLAG_EXACT) != 0;
+  s.order = (h->flags & SDG_FLAG_ORDER_GENERAL) ? kOrderGeneral : kOrderOpt1;
+  s.lift = f32 ? static_cast<const void*>(h->lift32) : h->lift64;
+  s.escale = f32 ? static_cast<const void*>(h->esc32) : h->esc64;
+  s.fscale = f32 ? static_cast<const void*>(h->fsc32) : h->fsc64;
+  s.Ne = h->Ne;
+  s.elem0 = 0;
+  s.nelem = h->Ne;
+  s.D = h->D.data();
+  s.stream = h->stream;
+  return s;
+}
+
+int launch_halo(sdg_handle* h, void* f, bool f32, cudaStream_t st) {
+  if (h->NhaloNode == 0) return SDG_OK;
+  const int threads = 256;
+  const int blocks = std::min((h->NhaloNode + threads - 1) / threads, 148 * 8);
+  const long base = static_cast<long>(h->Np) * h->Ne;
+  if (f32)
+    halo_kernel<float><<<blocks, threads, 0, st>>>(static_cast<float*>(f), h->hsrc,
+                                                   base, h->NhaloNode);
+  else
+    halo_kernel<double><<<blocks, threads, 0, st>>>(static_cast<double*>(f), h->hsrc,
+                                                    base, h->NhaloNode);
+  SDG_CUDA(cudaGetLastError());
+  return SDG_OK;
+}
+
+// Validates the verbatim tables of advect3d_eq_cal_tend against the
+// structured form the fused kernel uses, and builds the compressed tables.
+int compress_tables(sdg_handle* h, const int* VMapM, const int* VMapP,
+                    const int* hmap, const double* nfn, const double* Esc,
+                    const double* Fsc, std::vector<int>* pbh,
+                    std::vector<int>* pbd, std::vector<double>* esc,
+                    std::vector<double>* fsc) {
+  const int Nq = h->Nq, Nfp = Nq * Nq, Np = h->Np, NfpTot = h->NfpTot, Ne = h->Ne;
+  const long NEf = static_cast<long>(NfpTot) * Ne, NEp = static_cast<long>(Np) * Ne;
+  const long halo0 = static_cast<long>(Np) * Ne;   // first halo DOF, 0-based
+  pbh->assign(6L * Ne, 0);
+  pbd->assign(6L * Ne, 0);
+  esc->assign(3L * Ne, 0.0);
+  fsc->assign(6L * Ne, 0.0);
+  bool direct = true;
+  for (long e = 0; e < Ne; ++e) {
+    for (int d = 0; d < 3; ++d) {
+      const double* col = Esc + e * Np + d * NEp;
+      for (int n = 1; n < Np; ++n)
+        if (col[n] != col[0])
+          return fail(SDG_ERR_MESH, "Escale(:,%ld,%d) is not constant over the "
+                      "element", e + 1, d + 1);
+      (*esc)[3 * e + d] = col[0];
+    }
+    for (int f = 0; f < 6; ++f) {
+      const long s0 = f * Nfp + NfpTot * e;
+      for (int fp = 0; fp < Nfp; ++fp) {
+        const long s = s0 + fp;
+        if (VMapM[s] != face_node(Nq, f, fp) + 1 + e * Np)
+          return fail(SDG_ERR_MESH, "VMapM(%ld,%ld) is not the element's own face "
+                      "node", s0 - NfpTot * e + fp + 1, e + 1);
+        for (int d = 0; d < 3; ++d) {
+          const double want = (d == kFaceAxis[f]) ? kFaceSign[f] : 0.0;
+          if (nfn[s + d * NEf] != want)
+            return fail(SDG_ERR_MESH, "normal_fn of face %d of element %ld is not "
+                        "the axis-aligned normal", f + 1, e + 1);
+        }
+        if (Fsc[s] != Fsc[s0])
+          return fail(SDG_ERR_MESH, "Fscale is not constant over face %d of "
+                      "element %ld", f + 1, e + 1);
+      }
+      (*fsc)[6 * e + f] = Fsc[s0];
+      const int opp = kOppFace[f];
+      const long p1 = static_cast<long>(VMapP[s0]) - 1;  // 0-based
+      if (p1 < 0 || p1 >= static_cast<long>(Np) * h->NeA)
+        return fail(SDG_ERR_MESH, "VMapP(%d,%ld) = %ld out of range", f * Nfp + 1,
+                    e + 1, p1 + 1);
+      if (p1 < halo0) {
+        const long pb = p1 - face_node(Nq, opp, 0);
+        if (pb < 0 || pb % Np != 0)
+          return fail(SDG_ERR_MESH, "VMapP of face %d of element %ld does not "
+                      "point at the opposite face of one element", f + 1, e + 1);
+        for (int fp = 0; fp < Nfp; ++fp)
+          if (static_cast<long>(VMapP[s0 + fp]) - 1 != pb + face_node(Nq, opp, fp))
+            return fail(SDG_ERR_MESH, "VMapP of face %d of element %ld is not "
+                        "node-for-node the opposite face", f + 1, e + 1);
+        (*pbh)[6 * e + f] = static_cast<int>(pb);
+        (*pbd)[6 * e + f] = static_cast<int>(pb);
+      } else {
+        for (int fp = 0; fp < Nfp; ++fp)
+          if (static_cast<long>(VMapP[s0 + fp]) - 1 != p1 + fp)
+            return fail(SDG_ERR_MESH, "halo slots of face %d of element %ld are "
+                        "not contiguous", f + 1, e + 1);
+        if (p1 + Nfp > halo0 + h->NhaloNode)
+          return fail(SDG_ERR_MESH, "halo slots of face %d of element %ld exceed "
+                      "NhaloNode", f + 1, e + 1);
+        (*pbh)[6 * e + f] = static_cast<int>(-1 - p1);
+        // Direct mode: read the halo's source (the periodic neighbour) itself.
+        if (direct && hmap) {
+          const long h0 = p1 - halo0;
+          const long src0 = static_cast<long>(hmap[h0]) - 1;
+          const long pb = src0 - face_node(Nq, opp, 0);
+          bool ok = pb >= 0 && pb % Np == 0 && pb < static_cast<long>(Np) * Ne;
+          for (int fp = 0; ok && fp < Nfp; ++fp)
+            ok = static_cast<long>(hmap[h0 + fp]) - 1 == pb + face_node(Nq, opp, fp);
+          if (ok) (*pbd)[6 * e + f] = static_cast<int>(pb);
+          else direct = false;
+        } else {
+          direct = false;
+        }
+      }
+    }
+  }
+  h->direct_ok = direct;
+  return SDG_OK;
+}
+
+template <typename T>
+int upload(T** dst, const T* src, size_t n) {
+  int rc = SDG_OK;
+  *dst = dev_alloc<T>(n, &rc);
+  if (!*dst) return rc;
+  SDG_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return SDG_OK;
+}
+
+int ensure_state(sdg_handle* h) {
+  if (h->q0) return SDG_OK;
+  int rc = SDG_OK;
+  const size_t NA = static_cast<size_t>(h->Np) * h->NeA;
+  const size_t es = mixed(h) ? sizeof(float) : sizeof(double);
+  if (!(h->q0 = dev_alloc<double>(NA, &rc))) return rc;
+  if (!(h->qa = dev_alloc<char>(NA * es, &rc))) return rc;
+  if (!(h->qb = dev_alloc<char>(NA * es, &rc))) return rc;
+  for (int d = 0; d < 3; ++d)
+    if (!(h->vel[d] = dev_alloc<char>(NA * es, &rc))) return rc;
+  if (mixed(h))
+    for (int d = 0; d < 3; ++d)
+      if (!(h->vel64[d] = dev_alloc<double>(NA, &rc))) return rc;
+  SDG_CUDA(cudaMemsetAsync(h->q0, 0, NA * sizeof(double), h->stream));
+  return SDG_OK;
+}
+
+// Enqueues stage st (0..2) of one SSP-RK3 step on the handle's stream.
+// Stage 1: q1 = q0 + dt*L(q0); stage 2: q2 = 3/4 q0 + 1/4 (q1 + dt*L(q1));
+// stage 3: q0 <- 1/3 q0 + 2/3 (q2 + dt*L(q2))  (main.f90:58-74 with the
+// coefficients of mod_common.f90:29-30).  The step-start copy q0 = q of
+// main.f90:53-56 disappears: q0 is the step's input buffer.
+int enqueue_stage(sdg_handle* h, int st, double dt) {
+  const bool f32 = mixed(h);
+  const int* pb = h->direct_ok ? h->pb_direct : h->pb_halo;
+  const double ra[3] = {0.0, 0.75, 1.0 / 3.0};
+  const double rb[3] = {1.0, 0.25, 2.0 / 3.0};
+  const void* in[3] = {h->q0, h->qa, h->qb};
+  void* out[3] = {h->qa, h->qb, h->q0};
+  if (!h->direct_ok) {
+    const bool in32 = f32 && st > 0;
+    int rc = launch_halo(h, const_cast<void*>(in[st]), in32, h->stream);
+    if (rc) return rc;
+  }
+  LaunchSpec s = base_spec(h, f32);
+  s.kind = f32 ? (kStageMixed1 + st) : kStageF64;
+  s.q = in[st];
+  s.u = h->vel[0];
+  s.v = h->vel[1];
+  s.w = h->vel[2];
+  s.q0 = h->q0;
+  s.out = out[st];
+  s.pbase = pb;
+  s.rk_a = ra[st];
+  s.rk_b = rb[st];
+  s.dt = dt;
+  return launch_tend(s);
+}
+
+// Enqueues one SSP-RK3 step (main.f90:51-74) on the handle's stream.
+int enqueue_step(sdg_handle* h, double dt) {
+  for (int st = 0; st < 3; ++st) {
+    int rc = enqueue_stage(h, st, dt);
+    if (rc) return rc;
+  }
+  return SDG_OK;
+}
+
+int check_handle(sdg_handle* h) {
+  if (!h) return fail(SDG_ERR_ARG, "null handle");
+  SDG_CUDA(cudaSetDevice(h->dev));
+  return SDG_OK;
+}
+
+// Adds the device time of the last rk3 batch to its timer once the stream
+// has passed it.
+void account_rk(sdg_handle* h) {
+  if (!h->rk_pending) return;
+  float ms = 0;
+  if (cudaEventSynchronize(h->ev1) == cudaSuccess &&
+      cudaEventElapsedTime(&ms, h->ev0, h->ev1) == cudaSuccess)
+    h->t_rk += 1e-3 * ms;
+  h->rk_pending = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
+             int NhaloNode, const double* D1D, const double* Lift_mat,
+             const int* VMapM, const int* VMapP, const int* halo_src_map,
+             const double* normal_fn, const double* Escale,
+             const double* Fscale, int flags) {
+  if (!out) return fail(SDG_ERR_ARG, "sdg_init: null handle pointer");
+  *out = nullptr;
+  if (Nq < 2 || Nq > 16)
+    return fail(SDG_ERR_ARG, "Nq = %d: PolyOrder must be 1..15", Nq);
+  if (Np != Nq * Nq * Nq || NfpTot != 6 * Nq * Nq)
+    return fail(SDG_ERR_ARG, "Np/NfpTot inconsistent with Nq = %d", Nq);
+  if (Ne < 1 || NeA < Ne || NhaloNode < 0 ||
+      static_cast<long long>(Np) * NeA > 2147483647LL ||
+      static_cast<long long>(Np) * Ne + NhaloNode > static_cast<long long>(Np) * NeA)
+    return fail(SDG_ERR_ARG, "inconsistent sizes Ne=%d NeA=%d NhaloNode=%d", Ne,
+                NeA, NhaloNode);
+  if (!D1D || !Lift_mat || !VMapM || !VMapP || !normal_fn || !Escale || !Fscale ||
+      (NhaloNode > 0 && !halo_src_map))
+    return fail(SDG_ERR_ARG, "sdg_init: null array argument");
+  if (flags & ~(SDG_FLAG_EXACT | SDG_FLAG_ORDER_GENERAL | SDG_FLAG_MIXED))
+    return fail(SDG_ERR_ARG, "sdg_init: unknown flag bits 0x%x", flags);
+  if ((flags & SDG_FLAG_MIXED) && (flags & SDG_FLAG_EXACT))
+    return fail(SDG_ERR_ARG, "SDG_FLAG_EXACT applies to the FP64 form only");
+  sdg_handle* h = new sdg_handle();
+  h->Nq = Nq;
+  h->Np = Np;
+  h->NfpTot = NfpTot;
+  h->Ne = Ne;
+  h->NeA = NeA;
+  h->NhaloNode = NhaloNode;
+  h->flags = flags;
+  h->D.resize(Nq * Nq);
+  for (int i = 0; i < Nq; ++i)
+    for (int l = 0; l < Nq; ++l) h->D[i * Nq + l] = D1D[i + Nq * l];
+
+  std::vector<int> pbh, pbd;
+  std::vector<double> esc, fsc;
+  int rc = compress_tables(h, VMapM, VMapP, halo_src_map, normal_fn, Escale, Fscale,
+                           &pbh, &pbd, &esc, &fsc);
+  if (rc) { delete h; return rc; }
+  for (int b = 0; b < NhaloNode; ++b)
+    if (halo_src_map[b] < 1 || static_cast<long>(halo_src_map[b]) > static_cast<long>(Np) * Ne) {
+      delete h;
+      return fail(SDG_ERR_MESH, "halo_src_map(%d) = %d out of range", b + 1,
+                  halo_src_map[b]);
+    }
+  // The tables are valid; from here on a device is required.
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || ndev == 0) {
+    delete h;
+    return fail(SDG_ERR_CUDA, "no CUDA device available (%s); this library has no "
+                "CPU path", cudaGetErrorString(ce));
+  }
+  cudaGetDevice(&h->dev);
+
+  auto bail = [&](int code) { free_handle(h); return code; };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
+    return bail(fail(SDG_ERR_CUDA, "stream/event creation failed"));
+
+  std::vector<int> hs(NhaloNode);
+  for (int b = 0; b < NhaloNode; ++b) hs[b] = halo_src_map[b] - 1;
+  if ((rc = upload(&h->lift64, Lift_mat, 6L * Np)) ||
+      (rc = upload(&h->pb_halo, pbh.data(), pbh.size())) ||
+      (rc = upload(&h->pb_direct, pbd.data(), pbd.size())) ||
+      (rc = upload(&h->esc64, esc.data(), esc.size())) ||
+      (rc = upload(&h->fsc64, fsc.data(), fsc.size())) ||
+      (NhaloNode > 0 && (rc = upload(&h->hsrc, hs.data(), hs.size()))))
+    return bail(rc);
+  {
+    std::vector<float> l32(6L * Np), e32(esc.size()), f32v(fsc.size());
+    for (size_t i = 0; i < l32.size(); ++i) l32[i] = static_cast<float>(Lift_mat[i]);
+    for (size_t i = 0; i < e32.size(); ++i) e32[i] = static_cast<float>(esc[i]);
+    for (size_t i = 0; i < f32v.size(); ++i) f32v[i] = static_cast<float>(fsc[i]);
+    if ((rc = upload(&h->lift32, l32.data(), l32.size())) ||
+        (rc = upload(&h->esc32, e32.data(), e32.size())) ||
+        (rc = upload(&h->fsc32, f32v.data(), f32v.size())))
+      return bail(rc);
+  }
+  h->red_blocks = 148 * 4;
+  if (!(h->red_partials = dev_alloc<double>(2 * h->red_blocks, &rc)) ||
+      !(h->red_counter = dev_alloc<unsigned int>(1, &rc)) ||
+      !(h->red_result = dev_alloc<double>(2, &rc)) ||
+      !(h->lgl_wn = dev_alloc<double>(Np, &rc)))
+    return bail(rc);
+  if (cudaMemset(h->red_counter, 0, sizeof(unsigned int)) != cudaSuccess)
+    return bail(fail(SDG_ERR_CUDA, "cudaMemset failed"));
+  *out = h;
+  return SDG_OK;
+}
+
+int sdg_finalize(sdg_handle* h) {
+  if (!h) return fail(SDG_ERR_ARG, "null handle");
+  free_handle(h);
+  return SDG_OK;
+}
+
+int sdg_cal_tend_dev(sdg_handle* h, double* dqdt, const double* q,
+                     const double* u, const double* v, const double* w,
+                     void* stream) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!dqdt || !q || !u || !v || !w) return fail(SDG_ERR_ARG, "null device array");
+  LaunchSpec s = base_spec(h, false);
+  s.kind = kTendF64;
+  s.q = q;
+  s.u = u;
+  s.v = v;
+  s.w = w;
+  s.out = dqdt;
+  s.pbase = h->pb_halo;
+  if (stream) s.stream = static_cast<cudaStream_t>(stream);
+  rc = launch_tend(s);
+  if (!rc) ++h->launches;
+  return rc;
+}
+
+int sdg_cal_tend(sdg_handle* h, double* dqdt, const double* q,
+                 const double* u, const double* v, const double* w) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!dqdt || !q || !u || !v || !w) return fail(SDG_ERR_ARG, "null host array");
+  const size_t NA = static_cast<size_t>(h->Np) * h->NeA;
+  const size_t NE = static_cast<size_t>(h->Np) * h->Ne;
+  for (int i = 0; i < 5; ++i)
+    if (!h->io[i] && !(h->io[i] = dev_alloc<double>(NA, &rc))) return rc;
+  const double* src[4] = {q, u, v, w};
+  account_rk(h);
+  cudaEvent_t e2, e3;
+  SDG_CUDA(cudaEventCreate(&e2));
+  SDG_CUDA(cudaEventCreate(&e3));
+  SDG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  for (int i = 0; i < 4; ++i)
+    SDG_CUDA(cudaMemcpyAsync(h->io[i], src[i], NA * sizeof(double),
+                             cudaMemcpyHostToDevice, h->stream));
+  SDG_CUDA(cudaEventRecord(e2, h->stream));
+  rc = sdg_cal_tend_dev(h, h->io[4], h->io[0], h->io[1], h->io[2], h->io[3], nullptr);
+  if (rc) return rc;
+  SDG_CUDA(cudaEventRecord(e3, h->stream));
+  SDG_CUDA(cudaMemcpyAsync(dqdt, h->io[4], NE * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream));
+  SDG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  SDG_CUDA(cudaStreamSynchronize(h->stream));
+  float a = 0, b = 0, c = 0;
+  cudaEventElapsedTime(&a, h->ev0, e2);
+  cudaEventElapsedTime(&b, e2, e3);
+  cudaEventElapsedTime(&c, e3, h->ev1);
+  h->t_copy += 1e-3 * (a + c);
+  h->t_tend += 1e-3 * b;
+  cudaEventDestroy(e2);
+  cudaEventDestroy(e3);
+  return SDG_OK;
+}
+
+int sdg_update_halo_dev(sdg_handle* h, double* f, void* stream) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!f) return fail(SDG_ERR_ARG, "null device array");
+  return launch_halo(h, f, false, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+}
+
+int sdg_set_field(sdg_handle* h, int which, const double* host) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (which < SDG_FIELD_Q || which > SDG_FIELD_W || !host)
+    return fail(SDG_ERR_ARG, "sdg_set_field: bad field or null array");
+  if ((rc = ensure_state(h))) return rc;
+  const size_t NE = static_cast<size_t>(h->Np) * h->Ne;
+  const size_t NA = static_cast<size_t>(h->Np) * h->NeA;
+  if (which == SDG_FIELD_Q) {
+    SDG_CUDA(cudaMemcpyAsync(h->q0, host, NE * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    if ((rc = launch_halo(h, h->q0, false, h->stream))) return rc;
+    h->have_q = true;
+  } else {
+    const int d = which - SDG_FIELD_U;
+    double* dst = mixed(h) ? h->vel64[d] : static_cast<double*>(h->vel[d]);
+    SDG_CUDA(cudaMemcpyAsync(dst, host, NE * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    if ((rc = launch_halo(h, dst, false, h->stream))) return rc;
+    if (mixed(h)) {
+      to_f32_kernel<<<148 * 8, 256, 0, h->stream>>>(static_cast<float*>(h->vel[d]), dst,
+                                                    static_cast<long>(NA));
+      SDG_CUDA(cudaGetLastError());
+    }
+    h->have_vel[d] = true;
+  }
+  SDG_CUDA(cudaStreamSynchronize(h->stream));
+  return SDG_OK;
+}
+
+int sdg_get_field(sdg_handle* h, int which, double* host) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (which < SDG_FIELD_Q || which > SDG_FIELD_W || !host)
+    return fail(SDG_ERR_ARG, "sdg_get_field: bad field or null array");
+  if (!h->q0) return fail(SDG_ERR_STATE, "no resident state: call sdg_set_field first");
+  const size_t NE = static_cast<size_t>(h->Np) * h->Ne;
+  const double* src = h->q0;
+  if (which != SDG_FIELD_Q) {
+    const int d = which - SDG_FIELD_U;
+    src = mixed(h) ? h->vel64[d] : static_cast<const double*>(h->vel[d]);
+  }
+  SDG_CUDA(cudaMemcpyAsync(host, src, NE * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+  SDG_CUDA(cudaStreamSynchronize(h->stream));
+  return SDG_OK;
+}
+
+int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(SDG_ERR_ARG, "nsteps must be >= 0");
+  if (!h->have_q || !h->have_vel[0] || !h->have_vel[1] || !h->have_vel[2])
+    return fail(SDG_ERR_STATE, "upload q, u, v and w with sdg_set_field first");
+  if (nsteps == 0) return SDG_OK;
+  if (!h->graph || h->graph_dt != dt) {
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    cudaGraph_t g;
+    SDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_step(h, dt);
+    cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
+    if (rc) return rc;
+    if (ee != cudaSuccess)
+      return fail(SDG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ee));
+    ee = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ee != cudaSuccess)
+      return fail(SDG_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ee));
+    h->graph_dt = dt;
+  }
+  account_rk(h);
+  SDG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  for (int i = 0; i < nsteps; ++i) SDG_CUDA(cudaGraphLaunch(h->graph, h->stream));
+  SDG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  h->rk_pending = true;
+  h->launches += 3LL * nsteps;
+  return SDG_OK;
+}
+
+int sdg_rk3_stage(sdg_handle* h, int stage, double dt) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (stage < 1 || stage > 3) return fail(SDG_ERR_ARG, "stage must be 1..3");
+  if (!h->have_q || !h->have_vel[0] || !h->have_vel[1] || !h->have_vel[2])
+    return fail(SDG_ERR_STATE, "upload q, u, v and w with sdg_set_field first");
+  rc = enqueue_stage(h, stage - 1, dt);
+  if (!rc) ++h->launches;
+  return rc;
+}
+
+int sdg_get_stream(sdg_handle* h, void** stream) {
+  if (!h || !stream) return fail(SDG_ERR_ARG, "null argument");
+  *stream = h->stream;
+  return SDG_OK;
+}
+
+int sdg_synchronize(sdg_handle* h) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  SDG_CUDA(cudaStreamSynchronize(h->stream));
+  account_rk(h);
+  return SDG_OK;
+}
+
+int sdg_minmax(sdg_handle* h, double* qmin, double* qmax) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!h->have_q) return fail(SDG_ERR_STATE, "no resident state");
+  const long n = static_cast<long>(h->Np) * h->Ne;
+  minmax_kernel<<<h->red_blocks, kRedThreads, 0, h->stream>>>(
+      h->q0, n, h->red_partials, h->red_counter, h->red_result);
+  SDG_CUDA(cudaGetLastError());
+  double r[2];
+  SDG_CUDA(cudaMemcpyAsync(r, h->red_result, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+  SDG_CUDA(cudaStreamSynchronize(h->stream));
+  if (qmin) *qmin = r[0];
+  if (qmax) *qmax = r[1];
+  return SDG_OK;
+}
+
+int sdg_diagnostics(sdg_handle* h, const double* lgl_w, double jac, double* mass,
+                    double* l2) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!h->have_q) return fail(SDG_ERR_STATE, "no resident state");
+  if (!lgl_w) return fail(SDG_ERR_ARG, "null weights");
+  const int Nq = h->Nq;
+  std::vector<double> wn(h->Np);
+  for (int k = 0; k < Nq; ++k)
+    for (int j = 0; j < Nq; ++j)
+      for (int i = 0; i < Nq; ++i) wn[i + Nq * j + Nq * Nq * k] = lgl_w[i] * lgl_w[j] * lgl_w[k];
+  SDG_CUDA(cudaMemcpyAsync(h->lgl_wn, wn.data(), h->Np * sizeof(double),
+                           cudaMemcpyHostToDevice, h->stream));
+  const long n = static_cast<long>(h->Np) * h->Ne;
+  moments_kernel<<<h->red_blocks, kRedThreads, 0, h->stream>>>(
+      h->q0, h->lgl_wn, h->Np, n, jac, h->red_partials, h->red_counter, h->red_result);
+  SDG_CUDA(cudaGetLastError());
+  double r[2];
+  SDG_CUDA(cudaMemcpyAsync(r, h->red_result, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+  SDG_CUDA(cudaStreamSynchronize(h->stream));
+  if (mass) *mass = r[0];
+  if (l2) *l2 = std::sqrt(r[1]);
+  return SDG_OK;
+}
+
+int sdg_field_dev_ptr(sdg_handle* h, int which, void** ptr) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!ptr || which < SDG_FIELD_Q || which > SDG_FIELD_W)
+    return fail(SDG_ERR_ARG, "sdg_field_dev_ptr: bad argument");
+  if ((rc = ensure_state(h))) return rc;
+  *ptr = which == SDG_FIELD_Q ? static_cast<void*>(h->q0) : h->vel[which - SDG_FIELD_U];
+  return SDG_OK;
+}
+
+int sdg_timers(sdg_handle* h, double* t4) {
+  if (!h || !t4) return fail(SDG_ERR_ARG, "null argument");
+  account_rk(h);
+  t4[0] = h->t_tend;
+  t4[1] = h->t_rk;
+  t4[2] = h->t_halo;
+  t4[3] = h->t_copy;
+  return SDG_OK;
+}
+
+long long sdg_launch_count(sdg_handle* h) { return h ? h->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// Host-side launch description shared by the per-order instantiation units
+// (sdg_tend_inst.cu, compiled once per NQ) and the library core.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sdg {
+
+// Summation order of the contractions for NQ > 8: OPT1's three partial sums
+// (mod_dg_optr_kernel_opt1.F90.erb:242-274) or GENERAL's sequential loop
+// (mod_dg_optr_kernel.f90:221-257).  Identical for NQ <= 8.
+enum SumOrder { kOrderOpt1 = 0, kOrderGeneral = 1 };
+
+// Which typed variant of the fused kernel to run.
+enum TendKind {
+  kTendF64 = 0,       // dqdt = L(q), all FP64
+  kStageF64 = 1,      // q_new = a*q0 + b*(q + dt*L(q)), all FP64
+  kStageMixed1 = 2,   // FP64 q in, FP32 velocity/compute, FP32 q out
+  kStageMixed2 = 3,   // FP32 q in, FP64 q0, FP32 q out
+  kStageMixed3 = 4,   // FP32 q in, FP64 q0, FP64 q out
+};
+
+struct LaunchSpec {
+  int nq;
+  int kind;          // TendKind
+  bool exact;        // separate roundings, reference order (FP64 kinds)
+  int order;         // SumOrder (matters for exact FP64 and NQ > 8)
+  const void* q;
+  const void* u;
+  const void* v;
+  const void* w;
+  const double* q0;
+  void* out;
+  const void* lift;    // FP64 or FP32 by kind
+  const int* pbase;
+  const void* escale;
+  const void* fscale;
+  int Ne;
+  int elem0;
+  int nelem;
+  double rk_a, rk_b, dt;
+  const double* D;     // row-major D(i,l), NQ*NQ
+  cudaStream_t stream;
+};
+
+// Returns 0 when launched, -1 when this unit does not hold spec.nq,
+// otherwise a cudaError_t value.
+int launch_tend_nq2(const LaunchSpec&);
+int launch_tend_nq3(const LaunchSpec&);
+int launch_tend_nq4(const LaunchSpec&);
+int launch_tend_nq5(const LaunchSpec&);
+int launch_tend_nq6(const LaunchSpec&);
+int launch_tend_nq7(const LaunchSpec&);
+int launch_tend_nq8(const LaunchSpec&);
+int launch_tend_nq9(const LaunchSpec&);
+int launch_tend_nq10(const LaunchSpec&);
+int launch_tend_nq11(const LaunchSpec&);
+int launch_tend_nq12(const LaunchSpec&);
+int launch_tend_nq13(const LaunchSpec&);
+int launch_tend_nq14(const LaunchSpec&);
+int launch_tend_nq15(const LaunchSpec&);
+int launch_tend_nq16(const LaunchSpec&);
+
+// Shared-memory bytes and threads per block of the fused kernel.
+void tend_block_shape(int nq, bool fp32, int* threads, size_t* smem,
+                      int* elems_per_block);
+
+}  // namespace sdg

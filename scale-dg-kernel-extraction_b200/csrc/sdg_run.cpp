@@ -1,0 +1,250 @@
+// sdg_run: the reference driver (main.f90) over the B200 C ABI.
+//
+// Reads the &PARAM_ADVECT3D namelist of main.f90:103-107 from argv[1] with
+// the same defaults (main.f90:94-101,113-115), sets up the mesh and
+// operators, initialises the fields, runs the SSP-RK3 loop on the GPU and
+// prints the reference's "istep min max" lines (main.f90:76-79, format
+// (I8,2ES24.15)) and timer report (main.f90:169-181).
+//
+// DGOptrKernel_OptType (character(len=8), main.f90:101) selects the GPU
+// arithmetic:
+//   "GPU"     FMA contractions in OPT1 order (fastest; <= 1e-12 of the
+//             reference);
+//   "OPT1"    the reference's OPT1 rounding reproduced bit for bit on the GPU
+//             (no FMA, three partial sums for p > 7);
+//   "GENERAL" the reference's GENERAL rounding reproduced bit for bit.
+// Additive keys (reference input.conf files parse unchanged):
+//   GPU_Precision   "FP64" (default) or "MIXED" (FP32 tendency, FP64 RK)
+//   IC_kind         0: sine product of main.f90:149-151 (default)
+//                   1: seeded Gaussian + 8 Fourier modes
+//   IC_seed         seed of the IC stream (integer)
+//   Vel_kind        0: constant (vel_x, vel_y, vel_z) (default)
+//                   1: divergence-free (sin 2 pi y, sin 2 pi z, sin 2 pi x)
+//   OperatorDataDir directory of p<p>.dat (default "operator_data")
+//
+// Usage: sdg_run input.conf
+
+#include <cctype>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "sdg_gpu.h"
+
+namespace {
+
+std::string upper(std::string s) {
+  for (auto& c : s) c = static_cast<char>(std::toupper(static_cast<unsigned char>(c)));
+  return s;
+}
+
+std::string trim(const std::string& s) {
+  const size_t a = s.find_first_not_of(" \t\r\n");
+  if (a == std::string::npos) return std::string();
+  const size_t b = s.find_last_not_of(" \t\r\n");
+  return s.substr(a, b - a + 1);
+}
+
+// Namelist group reader: "&GROUP key = value, ... /" with '!' comments and
+// quoted strings.  Returns false when the group is absent or unterminated.
+bool read_group(const std::string& text, const std::string& group,
+                std::map<std::string, std::string>* kv, std::string* err) {
+  // Strip comments outside quotes.
+  std::string t;
+  bool inq = false, com = false;
+  char qc = 0;
+  for (char c : text) {
+    if (com) { if (c == '\n') { com = false; t += c; } continue; }
+    if (inq) { t += c; if (c == qc) inq = false; continue; }
+    if (c == '"' || c == '\'') { inq = true; qc = c; t += c; continue; }
+    if (c == '!') { com = true; continue; }
+    t += c;
+  }
+  const std::string tag = "&" + upper(group);
+  size_t p = upper(t).find(tag);
+  if (p == std::string::npos) { *err = "namelist group " + tag + " not found"; return false; }
+  p += tag.size();
+  std::string cur;
+  inq = false;
+  for (; p < t.size(); ++p) {
+    const char c = t[p];
+    const bool end = !inq && c == '/';
+    if (inq) { cur += c; if (c == qc) inq = false; continue; }
+    if (c == '"' || c == '\'') { inq = true; qc = c; cur += c; continue; }
+    if (end || c == ',' || c == '\n') {
+      const std::string item = trim(cur);
+      cur.clear();
+      if (!item.empty()) {
+        const size_t eq = item.find('=');
+        if (eq == std::string::npos) { *err = "bad namelist item: " + item; return false; }
+        std::string v = trim(item.substr(eq + 1));
+        if (v.size() >= 2 && (v[0] == '"' || v[0] == '\'')) v = v.substr(1, v.size() - 2);
+        (*kv)[upper(trim(item.substr(0, eq)))] = v;
+      }
+      if (end) return true;
+      continue;
+    }
+    cur += c;
+  }
+  *err = "namelist group " + tag + " is not terminated by '/'";
+  return false;
+}
+
+bool to_int(const std::string& s, int* out) {
+  char* e = nullptr;
+  const long v = std::strtol(s.c_str(), &e, 10);
+  if (e == s.c_str() || *e) return false;
+  *out = static_cast<int>(v);
+  return true;
+}
+
+bool to_real(std::string s, double* out) {
+  for (auto& c : s)
+    if (c == 'd' || c == 'D') c = 'E';
+  char* e = nullptr;
+  *out = std::strtod(s.c_str(), &e);
+  return e != s.c_str() && *e == '\0';
+}
+
+int die(const char* what) {
+  char buf[512];
+  sdg_last_error(buf, sizeof(buf));
+  std::fprintf(stderr, "Error: %s: %s\n", what, buf);
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc < 2) {
+    std::fprintf(stderr, "Error: configuration file argument is required.\n"
+                         "Usage: sdg_run input.conf\n");
+    return 1;
+  }
+  std::ifstream in(argv[1]);
+  if (!in) {
+    std::fprintf(stderr, "Error: cannot open %s\n", argv[1]);
+    return 1;
+  }
+  std::stringstream ss;
+  ss << in.rdbuf();
+  std::map<std::string, std::string> kv;
+  std::string err;
+  if (!read_group(ss.str(), "PARAM_ADVECT3D", &kv, &err)) {
+    std::fprintf(stderr, "Error: %s\n", err.c_str());
+    return 1;
+  }
+  int NeX = 4, NeY = 4, NeZ = 4, p = 3, nstep = 100, out_int = 10;
+  int ic_kind = 0, vel_kind = 0, seed = 0;
+  double vx = 1.0, vy = 1.0, vz = 1.0, dt = 1.0e-3;
+  std::string opt = "OPT1", prec = "FP64", opdir = "operator_data";
+  for (const auto& it : kv) {
+    const std::string& k = it.first;
+    const std::string& v = it.second;
+    bool ok = true;
+    if (k == "NEX") ok = to_int(v, &NeX);
+    else if (k == "NEY") ok = to_int(v, &NeY);
+    else if (k == "NEZ") ok = to_int(v, &NeZ);
+    else if (k == "POLYORDER") ok = to_int(v, &p);
+    else if (k == "DT") ok = to_real(v, &dt);
+    else if (k == "NSTEP") ok = to_int(v, &nstep);
+    else if (k == "OUTPUT_INTERVAL") ok = to_int(v, &out_int);
+    else if (k == "VEL_X") ok = to_real(v, &vx);
+    else if (k == "VEL_Y") ok = to_real(v, &vy);
+    else if (k == "VEL_Z") ok = to_real(v, &vz);
+    else if (k == "DGOPTRKERNEL_OPTTYPE") opt = upper(trim(v));
+    else if (k == "GPU_PRECISION") prec = upper(trim(v));
+    else if (k == "IC_KIND") ok = to_int(v, &ic_kind);
+    else if (k == "IC_SEED") ok = to_int(v, &seed);
+    else if (k == "VEL_KIND") ok = to_int(v, &vel_kind);
+    else if (k == "OPERATORDATADIR") opdir = v;
+    else {
+      std::fprintf(stderr, "Error: unknown namelist key %s in &PARAM_ADVECT3D\n", k.c_str());
+      return 1;
+    }
+    if (!ok) {
+      std::fprintf(stderr, "Error: bad value '%s' for %s\n", v.c_str(), k.c_str());
+      return 1;
+    }
+  }
+  int flags = 0;
+  if (opt == "GPU") flags = 0;
+  else if (opt == "OPT1") flags = SDG_FLAG_EXACT;
+  else if (opt == "GENERAL") flags = SDG_FLAG_EXACT | SDG_FLAG_ORDER_GENERAL;
+  else {
+    // The reference only prints this and leaves eval_typeid unset
+    // (mod_dg_optr_kernel.f90:54-55); here it is an error.
+    std::fprintf(stderr, "Error: Unsupported dgoptr_evaltype: %s\n", opt.c_str());
+    return 2;
+  }
+  if (prec == "MIXED") {
+    if (opt != "GPU") {
+      std::fprintf(stderr, "Error: GPU_Precision = MIXED needs DGOptrKernel_OptType = GPU\n");
+      return 2;
+    }
+    flags |= SDG_FLAG_MIXED;
+  } else if (prec != "FP64") {
+    std::fprintf(stderr, "Error: GPU_Precision must be FP64 or MIXED\n");
+    return 2;
+  }
+  if (out_int <= 0) {
+    std::fprintf(stderr, "Error: output_interval must be positive\n");
+    return 1;
+  }
+
+  int sz[6];
+  if (sdg_mesh_sizes(NeX, NeY, NeZ, p, sz)) return die("mesh_setup");
+  const int Ne = sz[0], NeA = sz[2], NhaloNode = sz[3], Np = sz[4], NfpTot = sz[5];
+  const int Nq = p + 1;
+  std::vector<double> x1D(Nq), D1D(Nq * Nq), Lift(6L * Np);
+  if (sdg_read_operators(opdir.c_str(), p, x1D.data(), D1D.data(), Lift.data()))
+    return die("element_init");
+  const size_t NEf = static_cast<size_t>(NfpTot) * Ne, NEp = static_cast<size_t>(Np) * Ne;
+  std::vector<int> VMapM(NEf), VMapP(NEf), hmap(NhaloNode);
+  std::vector<double> nfn(3 * NEf), Esc(3 * NEp), Fsc(NEf), pos(3 * NEp);
+  if (sdg_mesh_setup(NeX, NeY, NeZ, p, 1.0, 1.0, 1.0, x1D.data(), VMapM.data(),
+                     VMapP.data(), hmap.data(), nfn.data(), Esc.data(), Fsc.data(),
+                     pos.data()))
+    return die("mesh_setup");
+  sdg_handle* h = nullptr;
+  if (sdg_init(&h, Nq, Np, NfpTot, Ne, NeA, NhaloNode, D1D.data(), Lift.data(),
+               VMapM.data(), VMapP.data(), hmap.data(), nfn.data(), Esc.data(),
+               Fsc.data(), flags))
+    return die("sdg_init");
+  std::vector<double> q(NEp), u(NEp), v(NEp), w(NEp);
+  if (sdg_init_fields(ic_kind, static_cast<unsigned long long>(seed), vel_kind, vx, vy, vz,
+                      pos.data(), Np, Ne, q.data(), u.data(), v.data(), w.data()))
+    return die("initial condition");
+  if (sdg_set_field(h, SDG_FIELD_Q, q.data()) || sdg_set_field(h, SDG_FIELD_U, u.data()) ||
+      sdg_set_field(h, SDG_FIELD_V, v.data()) || sdg_set_field(h, SDG_FIELD_W, w.data()))
+    return die("upload");
+
+  const auto t0 = std::chrono::steady_clock::now();
+  int done = 0;
+  while (done < nstep) {
+    const int next = std::min(nstep, (done / out_int + 1) * out_int);
+    if (sdg_rk3_steps(h, dt, next - done)) return die("rk3");
+    done = next;
+    if (done % out_int == 0) {
+      double mn, mx;
+      if (sdg_minmax(h, &mn, &mx)) return die("minmax");
+      std::printf("%8d%24.15E%24.15E\n", done, mn, mx);
+    }
+  }
+  if (sdg_synchronize(h)) return die("synchronize");
+  const double t_main =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  double tm[4];
+  sdg_timers(h, tm);
+  std::printf("= Report of execution time [sec]\n");
+  std::printf("%30s%24.5E\n", "Main:", t_main);
+  std::printf("%30s%24.5E\n", "Cal_tend:", tm[1]);
+  std::printf("%30s%24.5E\n", "Fused flux+dqdt+RK stage:", tm[1]);
+  sdg_finalize(h);
+  return 0;
+}

@@ -1,0 +1,81 @@
+// Instantiates the fused tendency kernel for one polynomial order.
+// Compiled once per NQ = p+1 (2..16) with -DSDG_NQ=<NQ>, so the fifteen
+// fully unrolled variants build in parallel.
+#include "sdg_launch.h"
+#include "sdg_tend.cuh"
+
+#ifndef SDG_NQ
+#error "SDG_NQ must be defined"
+#endif
+
+namespace sdg {
+namespace {
+
+constexpr int NQ = SDG_NQ;
+
+template <typename TQ, typename TV, typename TO, typename TC, bool EXACT,
+          int ORDER, bool STAGE>
+int run(const LaunchSpec& s) {
+  using G = Geo<NQ>;
+  TendArgs<TQ, TV, TO, TC> a;
+  a.q = static_cast<const TQ*>(s.q);
+  a.u = static_cast<const TV*>(s.u);
+  a.v = static_cast<const TV*>(s.v);
+  a.w = static_cast<const TV*>(s.w);
+  a.q0 = s.q0;
+  a.out = static_cast<TO*>(s.out);
+  a.lift = static_cast<const TC*>(s.lift);
+  a.pbase = s.pbase;
+  a.escale = static_cast<const TC*>(s.escale);
+  a.fscale = static_cast<const TC*>(s.fscale);
+  a.Ne = s.Ne;
+  a.elem0 = s.elem0;
+  a.nelem = s.nelem;
+  a.rk_a = s.rk_a;
+  a.rk_b = s.rk_b;
+  a.dt = s.dt;
+  DMat<NQ, TC> d;
+  for (int i = 0; i < NQ * NQ; ++i) d.d[i] = static_cast<TC>(s.D[i]);
+  auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
+  const size_t smem = SmemLayout<NQ, TC>::BYTES;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return static_cast<int>(e);
+  }
+  if (s.nelem <= 0) return 0;
+  const int blocks = (s.nelem + G::EPB - 1) / G::EPB;
+  kern<<<blocks, G::THREADS, smem, s.stream>>>(a, d);
+  return static_cast<int>(cudaGetLastError());
+}
+
+}  // namespace
+
+#define SDG_CAT2(a, b) a##b
+#define SDG_CAT(a, b) SDG_CAT2(a, b)
+
+int SDG_CAT(launch_tend_nq, SDG_NQ)(const LaunchSpec& s) {
+  if (s.nq != NQ) return -1;
+  // Orders only differ for NQ > 8; below that both map to one variant.
+  const bool gen = (NQ > 8) && s.order == kOrderGeneral;
+  switch (s.kind) {
+    case kTendF64:
+      if (!s.exact) return run<double, double, double, double, false, kOrderOpt1, false>(s);
+      if (gen) return run<double, double, double, double, true, kOrderGeneral, false>(s);
+      return run<double, double, double, double, true, kOrderOpt1, false>(s);
+    case kStageF64:
+      if (!s.exact) return run<double, double, double, double, false, kOrderOpt1, true>(s);
+      if (gen) return run<double, double, double, double, true, kOrderGeneral, true>(s);
+      return run<double, double, double, double, true, kOrderOpt1, true>(s);
+    case kStageMixed1:
+      return run<double, float, float, float, false, kOrderOpt1, true>(s);
+    case kStageMixed2:
+      return run<float, float, float, float, false, kOrderOpt1, true>(s);
+    case kStageMixed3:
+      return run<float, float, double, float, false, kOrderOpt1, true>(s);
+    default:
+      return static_cast<int>(cudaErrorInvalidValue);
+  }
+}
+
+}  // namespace sdg

@@ -1,0 +1,381 @@
+"""Python binding of the B200 SCALE-DG advection library (libsdg_gpu.so).
+
+A thin ctypes layer over the C ABI declared in include/sdg_gpu.h.  Arrays
+use the reference's Fortran layout: numpy arrays in column-major order
+(``order="F"``) with the reference's shapes, e.g. ``q`` is ``(Np, NeA)``,
+``VMapM`` is ``(NfpTot, Ne)`` and holds 1-based indices.
+
+The module mirrors the reference's driver surface:
+
+* ``dg_optr_kernel_setup(evaltype)`` - the selector of
+  mod_dg_optr_kernel.f90:45-58; "GPU" picks the fast FMA kernels, "OPT1" and
+  "GENERAL" reproduce those CPU kernels' rounding bit for bit on the GPU;
+* ``advect3d_eq_cal_tend(dqdt, q, u, v, w, D1D, D1D_tr, Lift_mat, VMapM,
+  VMapP, normal_fn, Escale, Fscale, Nq, Np, NfpTot, Ne, NeA)`` - the
+  tendency call of mod_advect3d_eq.f90:41-85 with the same arguments;
+* ``mesh_setup`` / ``read_operators`` / ``update_halo`` - mod_mesh.f90.
+
+There is no CPU path: every compute call runs the CUDA library, and a
+missing library or device raises ``SdgError``.
+"""
+
+import ctypes
+import os
+from collections import namedtuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.dirname(_HERE)
+REPO_DIR = os.path.dirname(PKG_DIR)
+LIB_PATH = os.path.join(PKG_DIR, "libsdg_gpu.so")
+OPERATOR_DIR = os.path.join(REPO_DIR, "operator_data")
+
+SDG_OK = 0
+SDG_ERR_ARG = 1
+SDG_ERR_CUDA = 2
+SDG_ERR_IO = 3
+SDG_ERR_MESH = 4
+SDG_ERR_STATE = 5
+
+FLAG_EXACT = 1
+FLAG_ORDER_GENERAL = 2
+FLAG_MIXED = 4
+
+FIELD_Q, FIELD_U, FIELD_V, FIELD_W = 0, 1, 2, 3
+
+# Exported symbols and their signatures (must match include/sdg_gpu.h).
+_I, _D, _P, _LL = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
+_U64 = ctypes.c_ulonglong
+SIGNATURES = {
+    "sdg_last_error": (_I, [ctypes.c_char_p, _I]),
+    "sdg_version": (ctypes.c_char_p, []),
+    "sdg_read_operators": (_I, [ctypes.c_char_p, _I, _P, _P, _P]),
+    "sdg_mesh_sizes": (_I, [_I, _I, _I, _I, _P]),
+    "sdg_fmask": (_I, [_I, _P]),
+    "sdg_mesh_setup": (_I, [_I, _I, _I, _I, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "sdg_update_halo_host": (_I, [_P, _I, _I, _I, _P]),
+    "sdg_init_fields": (_I, [_I, _U64, _I, _D, _D, _D, _P, _I, _I, _P, _P, _P, _P]),
+    "sdg_random_velocity": (_I, [_U64, _P]),
+    "sdg_init": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P,
+                      _P, _P, _P, _I]),
+    "sdg_finalize": (_I, [_P]),
+    "sdg_cal_tend": (_I, [_P, _P, _P, _P, _P, _P]),
+    "sdg_cal_tend_dev": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "sdg_update_halo_dev": (_I, [_P, _P, _P]),
+    "sdg_set_field": (_I, [_P, _I, _P]),
+    "sdg_get_field": (_I, [_P, _I, _P]),
+    "sdg_rk3_steps": (_I, [_P, _D, _I]),
+    "sdg_minmax": (_I, [_P, _P, _P]),
+    "sdg_diagnostics": (_I, [_P, _P, _D, _P, _P]),
+    "sdg_synchronize": (_I, [_P]),
+    "sdg_rk3_stage": (_I, [_P, _I, _D]),
+    "sdg_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
+    "sdg_field_dev_ptr": (_I, [_P, _I, ctypes.POINTER(_P)]),
+    "sdg_timers": (_I, [_P, _P]),
+    "sdg_launch_count": (_LL, [_P]),
+}
+
+
+class SdgError(RuntimeError):
+    """A failed library call; ``code`` is the SDG_ERR_* status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[sdg status {code}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Loads libsdg_gpu.so once; raises SdgError when it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SdgError(SDG_ERR_CUDA, f"{LIB_PATH} is not built (run build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != SDG_OK:
+        buf = ctypes.create_string_buffer(1024)
+        lib().sdg_last_error(buf, 1024)
+        raise SdgError(rc, buf.value.decode(errors="replace"))
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _f64(a, shape=None):
+    a = np.asarray(a, dtype=np.float64, order="F")
+    if shape is not None and a.size != int(np.prod(shape)):
+        raise SdgError(SDG_ERR_ARG, f"array of {a.size} values where {shape} expected")
+    return a
+
+
+def _i32(a):
+    return np.asarray(a, dtype=np.int32, order="F")
+
+
+# ---------------------------------------------------------------------------
+# Host set-up (mod_mesh.f90)
+# ---------------------------------------------------------------------------
+Operators = namedtuple("Operators", "p Nq x1D D1D D1D_tr Lift_mat")
+Mesh = namedtuple(
+    "Mesh",
+    "NeX NeY NeZ p Nq Np Nfp NfpTot Ne Nhalo NeA NhaloNode "
+    "VMapM VMapP halo_src_map normal_fn Escale Fscale pos_en",
+)
+
+
+def read_operators(p, opdir=OPERATOR_DIR):
+    """element_init operator read (mod_mesh.f90:253-263)."""
+    Nq = p + 1
+    x1D = np.zeros(Nq)
+    D1D = np.zeros((Nq, Nq), order="F")
+    Lift = np.zeros((Nq, Nq, Nq, 6), order="F")
+    _check(lib().sdg_read_operators(opdir.encode(), p, _p(x1D), _p(D1D), _p(Lift)))
+    return Operators(p, Nq, x1D, D1D, np.asfortranarray(D1D.T), Lift)
+
+
+def mesh_sizes(NeX, NeY, NeZ, p):
+    s = np.zeros(6, dtype=np.int32)
+    _check(lib().sdg_mesh_sizes(NeX, NeY, NeZ, p, _p(s)))
+    return dict(zip(["Ne", "Nhalo", "NeA", "NhaloNode", "Np", "NfpTot"], map(int, s)))
+
+
+def fmask(p):
+    Nq = p + 1
+    F = np.zeros((Nq * Nq, 6), dtype=np.int32, order="F")
+    _check(lib().sdg_fmask(p, _p(F)))
+    return F
+
+
+def mesh_setup(NeX, NeY, NeZ, p, x1D, dom=(1.0, 1.0, 1.0)):
+    """mesh_setup (mod_mesh.f90:74-193): all tables, reference layout."""
+    s = mesh_sizes(NeX, NeY, NeZ, p)
+    Ne, NfpTot, Np = s["Ne"], s["NfpTot"], s["Np"]
+    VMapM = np.zeros((NfpTot, Ne), dtype=np.int32, order="F")
+    VMapP = np.zeros((NfpTot, Ne), dtype=np.int32, order="F")
+    hmap = np.zeros(s["NhaloNode"], dtype=np.int32)
+    nfn = np.zeros((NfpTot, Ne, 3), order="F")
+    Esc = np.zeros((Np, Ne, 3), order="F")
+    Fsc = np.zeros((NfpTot, Ne), order="F")
+    pos = np.zeros((Np, Ne, 3), order="F")
+    x1D = _f64(x1D)
+    _check(lib().sdg_mesh_setup(NeX, NeY, NeZ, p, dom[0], dom[1], dom[2], _p(x1D),
+                                _p(VMapM), _p(VMapP), _p(hmap), _p(nfn), _p(Esc),
+                                _p(Fsc), _p(pos)))
+    Nq = p + 1
+    return Mesh(NeX, NeY, NeZ, p, Nq, Np, Nq * Nq, NfpTot, Ne, s["Nhalo"], s["NeA"],
+                s["NhaloNode"], VMapM, VMapP, hmap, nfn, Esc, Fsc, pos)
+
+
+def update_halo(f, mesh):
+    """update_halo (mod_mesh.f90:209-221) on a host array, in place."""
+    if not (isinstance(f, np.ndarray) and f.dtype == np.float64 and
+            (f.flags.f_contiguous or f.flags.c_contiguous and f.ndim == 1)):
+        raise SdgError(SDG_ERR_ARG, "update_halo needs a contiguous float64 array")
+    _check(lib().sdg_update_halo_host(_p(f), mesh.Np, mesh.Ne, mesh.NhaloNode,
+                                      _p(mesh.halo_src_map)))
+    return f
+
+
+def init_fields(mesh, ic_kind=0, seed=0, vel_kind=0, vel=(1.0, 1.0, 1.0)):
+    """Initial q,u,v,w(Np,NeA) with halos filled (main.f90:146-162)."""
+    shape = (mesh.Np, mesh.NeA)
+    q, u, v, w = (np.zeros(shape, order="F") for _ in range(4))
+    _check(lib().sdg_init_fields(ic_kind, seed, vel_kind, vel[0], vel[1], vel[2],
+                                 _p(mesh.pos_en), mesh.Np, mesh.Ne, _p(q), _p(u),
+                                 _p(v), _p(w)))
+    for f in (q, u, v, w):
+        update_halo(f, mesh)
+    return q, u, v, w
+
+
+def random_velocity(seed):
+    out = np.zeros(3)
+    _check(lib().sdg_random_velocity(seed, _p(out)))
+    return out
+
+
+def lgl_weights(x1D):
+    """LGL quadrature weights w_i = 2 / (N (N+1) P_N(x_i)^2), N = Nq-1."""
+    N = len(x1D) - 1
+    PN = np.polynomial.legendre.legval(np.asarray(x1D), [0] * N + [1])
+    return 2.0 / (N * (N + 1) * PN ** 2)
+
+
+# ---------------------------------------------------------------------------
+# Handle
+# ---------------------------------------------------------------------------
+class Handle:
+    """Operators and mesh resident on the GPU (sdg_init ... sdg_finalize)."""
+
+    def __init__(self, ops, mesh, flags=0):
+        self._h = ctypes.c_void_p()
+        self.ops, self.mesh, self.flags = ops, mesh, flags
+        m = mesh
+        _check(lib().sdg_init(ctypes.byref(self._h), m.Nq, m.Np, m.NfpTot, m.Ne, m.NeA,
+                              m.NhaloNode, _p(_f64(ops.D1D)), _p(_f64(ops.Lift_mat)),
+                              _p(_i32(m.VMapM)), _p(_i32(m.VMapP)),
+                              _p(_i32(m.halo_src_map)), _p(_f64(m.normal_fn)),
+                              _p(_f64(m.Escale)), _p(_f64(m.Fscale)), flags))
+
+    @property
+    def ptr(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            _check(lib().sdg_finalize(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def cal_tend(self, q, u, v, w, dqdt=None):
+        """Drop-in tendency on host arrays (Np,NeA) -> dqdt (Np,NeA)."""
+        m = self.mesh
+        shape = (m.Np, m.NeA)
+        q, u, v, w = (_f64(a, shape) for a in (q, u, v, w))
+        if dqdt is None:
+            dqdt = np.zeros(shape, order="F")
+        _check(lib().sdg_cal_tend(self._h, _p(dqdt), _p(q), _p(u), _p(v), _p(w)))
+        return dqdt
+
+    def cal_tend_dev(self, dqdt, q, u, v, w, stream=None):
+        """Tendency on device tensors (anything with data_ptr())."""
+        _check(lib().sdg_cal_tend_dev(self._h, dqdt.data_ptr(), q.data_ptr(), u.data_ptr(),
+                                      v.data_ptr(), w.data_ptr(), stream))
+
+    def update_halo_dev(self, f, stream=None):
+        _check(lib().sdg_update_halo_dev(self._h, f.data_ptr(), stream))
+
+    def set_field(self, which, host):
+        host = _f64(host)
+        if host.size < self.mesh.Np * self.mesh.Ne:
+            raise SdgError(SDG_ERR_ARG, "field smaller than (Np, Ne)")
+        _check(lib().sdg_set_field(self._h, which, _p(host)))
+
+    def set_state(self, q, u, v, w):
+        for which, a in zip((FIELD_Q, FIELD_U, FIELD_V, FIELD_W), (q, u, v, w)):
+            self.set_field(which, a)
+
+    def get_field(self, which=FIELD_Q):
+        out = np.zeros((self.mesh.Np, self.mesh.Ne), order="F")
+        _check(lib().sdg_get_field(self._h, which, _p(out)))
+        return out
+
+    def rk3_steps(self, dt, nsteps):
+        _check(lib().sdg_rk3_steps(self._h, dt, nsteps))
+
+    def rk3_stage(self, stage, dt):
+        """One stage (1..3) of an RK3 step, without a graph."""
+        _check(lib().sdg_rk3_stage(self._h, stage, dt))
+
+    def stream(self):
+        """The handle's cudaStream_t as an integer."""
+        s = ctypes.c_void_p()
+        _check(lib().sdg_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def synchronize(self):
+        _check(lib().sdg_synchronize(self._h))
+
+    def minmax(self):
+        mn, mx = ctypes.c_double(), ctypes.c_double()
+        _check(lib().sdg_minmax(self._h, ctypes.byref(mn), ctypes.byref(mx)))
+        return mn.value, mx.value
+
+    def diagnostics(self, lgl_w, jac):
+        w = _f64(lgl_w)
+        mass, l2 = ctypes.c_double(), ctypes.c_double()
+        _check(lib().sdg_diagnostics(self._h, _p(w), jac, ctypes.byref(mass),
+                                     ctypes.byref(l2)))
+        return mass.value, l2.value
+
+    def field_dev_ptr(self, which):
+        p = ctypes.c_void_p()
+        _check(lib().sdg_field_dev_ptr(self._h, which, ctypes.byref(p)))
+        return p.value
+
+    def timers(self):
+        t = np.zeros(4)
+        _check(lib().sdg_timers(self._h, _p(t)))
+        return t
+
+    def launch_count(self):
+        return int(lib().sdg_launch_count(self._h))
+
+
+# ---------------------------------------------------------------------------
+# The reference's operator/driver surface
+# ---------------------------------------------------------------------------
+_EVALTYPES = {"GPU": 0, "OPT1": FLAG_EXACT, "GENERAL": FLAG_EXACT | FLAG_ORDER_GENERAL}
+_eval_flags = None
+_handles = {}
+
+
+def dg_optr_kernel_setup(evaltype):
+    """Selector of mod_dg_optr_kernel.f90:45-58.  Unknown types raise (the
+    reference only prints and leaves the type unset, kern:54-55)."""
+    global _eval_flags
+    key = str(evaltype).strip().upper()
+    if key not in _EVALTYPES:
+        raise SdgError(SDG_ERR_ARG, f"Unsupported dgoptr_evaltype: {evaltype}")
+    _eval_flags = _EVALTYPES[key]
+
+
+def advect3d_eq_cal_tend(dqdt, q, u, v, w, D1D, D1D_tr, Lift_mat, VMapM, VMapP,
+                         normal_fn, Escale, Fscale, Nq, Np, NfpTot, Ne, NeA,
+                         halo_src_map=None):
+    """advect3d_eq_cal_tend (mod_advect3d_eq.f90:41-85) on the GPU.
+
+    Same arguments and meaning as the reference: writes dqdt(:,1:Ne) from
+    q,u,v,w(Np,NeA), reading the plus side through VMapP (halo included).
+    The device tables are built on first use for a given mesh and cached.
+    """
+    if _eval_flags is None:
+        raise SdgError(SDG_ERR_STATE, "call dg_optr_kernel_setup first")
+    if D1D_tr is not None and not np.array_equal(np.asarray(D1D_tr), np.asarray(D1D).T):
+        raise SdgError(SDG_ERR_ARG, "D1D_tr is not the transpose of D1D")
+    key = (id(VMapM), id(VMapP), id(Lift_mat), id(D1D), Nq, Ne, NeA, _eval_flags)
+    h = _handles.get(key)
+    if h is None:
+        NhaloNode = 0 if halo_src_map is None else int(np.asarray(halo_src_map).size)
+        ops = Operators(Nq - 1, Nq, None, _f64(D1D), None, _f64(Lift_mat))
+        mesh = Mesh(None, None, None, Nq - 1, Nq, Np, Nq * Nq, NfpTot, Ne, None, NeA,
+                    NhaloNode, _i32(VMapM), _i32(VMapP),
+                    _i32(halo_src_map if halo_src_map is not None else np.zeros(0)),
+                    _f64(normal_fn), _f64(Escale), _f64(Fscale), None)
+        h = Handle(ops, mesh, _eval_flags)
+        _handles[key] = (h, (VMapM, VMapP, Lift_mat, D1D))
+    else:
+        h = h[0]
+    out = h.cal_tend(q, u, v, w)
+    dqdt[:, :Ne] = out[:, :Ne]
+    return dqdt
+
+
+class Problem:
+    """Operators + mesh + handle for a periodic unit-cube run."""
+
+    def __init__(self, NeX, NeY, NeZ, p, flags=0, opdir=OPERATOR_DIR):
+        self.ops = read_operators(p, opdir)
+        self.mesh = mesh_setup(NeX, NeY, NeZ, p, self.ops.x1D)
+        self.handle = Handle(self.ops, self.mesh, flags)
+
+    def close(self):
+        self.handle.close()

@@ -1,0 +1,190 @@
+"""GPU parity against the CPU oracle, through the C ABI (needs a B200).
+
+T6  one tendency evaluation, p = 1..15: the fast FMA kernels agree with the
+    oracle's OPT1 to <= 1e-12 relative max-norm; the exact kernels equal the
+    oracle's OPT1 and GENERAL bit for bit.
+    The plus side is read through the caller's halo buffer exactly where
+    VMapP points (a stale halo gives the oracle's answer on the same input).
+T7  trajectories of the resident RK3 path: <= 1e-12 (fast), bit for bit
+    (exact), after many steps.
+T10 mixed precision: relative L2 error <= 1e-5 against the FP64 oracle.
+Plus the device-pointer entry point, min/max and the FP64 diagnostics.
+"""
+import numpy as np
+import pytest
+
+import orc
+import sdg_b200 as sdg
+from conftest import rel_maxnorm
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build(built):
+    return built
+
+
+def dims_for(p):
+    return (3, 4, 2) if p <= 5 else ((3, 2, 2) if p <= 9 else (2, 2, 2))
+
+
+def case(p, dims=None, seed=11, vel_kind=1, ic_kind=1):
+    dims = dims or dims_for(p)
+    ops = sdg.read_operators(p)
+    mesh = sdg.mesh_setup(*dims, p, ops.x1D)
+    omesh = orc.mesh_setup(*dims, p, ops.x1D)
+    q, u, v, w = sdg.init_fields(mesh, ic_kind=ic_kind, seed=seed, vel_kind=vel_kind,
+                                 vel=(1.0, 0.5, 0.25))
+    return ops, mesh, omesh, (q, u, v, w)
+
+
+@pytest.mark.parametrize("p", range(1, 16))
+def test_rhs_fast_vs_oracle(p):
+    ops, mesh, omesh, (q, u, v, w) = case(p)
+    h = sdg.Handle(ops, mesh, 0)
+    got = h.cal_tend(q, u, v, w)[:, : mesh.Ne]
+    ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+    assert rel_maxnorm(got, ref) <= TOL
+    h.close()
+
+
+@pytest.mark.parametrize("p", range(1, 16))
+@pytest.mark.parametrize("order", ["OPT1", "GENERAL"])
+def test_rhs_exact_bitwise(p, order):
+    ops, mesh, omesh, (q, u, v, w) = case(p)
+    flags = sdg.FLAG_EXACT | (sdg.FLAG_ORDER_GENERAL if order == "GENERAL" else 0)
+    h = sdg.Handle(ops, mesh, flags)
+    got = h.cal_tend(q, u, v, w)[:, : mesh.Ne]
+    ev = orc.OPT1 if order == "OPT1" else orc.GENERAL
+    ref = orc.cal_tend(ev, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+    assert np.array_equal(got, ref), rel_maxnorm(got, ref)
+    h.close()
+
+
+def test_halo_buffer_is_read_through_vmapp():
+    """Random values in the halo region (no update_halo): the GPU reads them
+    where VMapP points, exactly like the reference."""
+    p = 4
+    ops, mesh, omesh, (q, u, v, w) = case(p)
+    rng = np.random.default_rng(5)
+    base = mesh.Np * mesh.Ne
+    qf = q.reshape(-1, order="F")
+    qf[base: base + mesh.NhaloNode] = rng.standard_normal(mesh.NhaloNode)
+    h = sdg.Handle(ops, mesh, sdg.FLAG_EXACT)
+    got = h.cal_tend(q, u, v, w)[:, : mesh.Ne]
+    ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+    assert np.array_equal(got, ref)
+    h.close()
+
+
+def test_reference_call_surface():
+    """advect3d_eq_cal_tend with the reference's argument list."""
+    p = 3
+    ops, mesh, omesh, (q, u, v, w) = case(p)
+    sdg.dg_optr_kernel_setup("OPT1")
+    dqdt = np.zeros_like(q)
+    m = mesh
+    sdg.advect3d_eq_cal_tend(dqdt, q, u, v, w, ops.D1D, ops.D1D_tr, ops.Lift_mat,
+                             m.VMapM, m.VMapP, m.normal_fn, m.Escale, m.Fscale,
+                             m.Nq, m.Np, m.NfpTot, m.Ne, m.NeA, m.halo_src_map)
+    ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)
+    assert np.array_equal(dqdt[:, : m.Ne], ref[:, : m.Ne])
+
+
+def run_both(p, dims, nstep, flags, ev=orc.OPT1, vel_kind=1):
+    ops, mesh, omesh, (q, u, v, w) = case(p, dims, vel_kind=vel_kind)
+    h = 1.0 / max(dims)
+    dt = 0.1 * h / (p + 1) ** 2
+    H = sdg.Handle(ops, mesh, flags)
+    H.set_state(q, u, v, w)
+    H.rk3_steps(dt, nstep)
+    got = H.get_field()
+    qo = q.copy(order="F")
+    orc.run_rk3(ev, qo, u, v, w, ops, omesh, dt, nstep)
+    H.close()
+    return got, qo[:, : mesh.Ne]
+
+
+@pytest.mark.parametrize("p,dims,nstep", [(1, (4, 3, 2), 40), (3, (4, 4, 3), 30),
+                                          (7, (3, 2, 4), 20), (10, (2, 2, 2), 8)])
+def test_trajectory_fast(p, dims, nstep):
+    got, ref = run_both(p, dims, nstep, 0)
+    assert rel_maxnorm(got, ref) <= TOL
+
+
+@pytest.mark.parametrize("p,dims,nstep,order",
+                         [(2, (3, 4, 2), 25, "OPT1"), (7, (2, 3, 2), 12, "OPT1"),
+                          (9, (2, 2, 2), 6, "GENERAL"), (9, (2, 2, 2), 6, "OPT1")])
+def test_trajectory_exact_bitwise(p, dims, nstep, order):
+    flags = sdg.FLAG_EXACT | (sdg.FLAG_ORDER_GENERAL if order == "GENERAL" else 0)
+    ev = orc.GENERAL if order == "GENERAL" else orc.OPT1
+    got, ref = run_both(p, dims, nstep, flags, ev)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("p,dims,nstep", [(7, (4, 4, 4), 50), (15, (2, 2, 2), 20)])
+def test_mixed_precision_error(p, dims, nstep):
+    got, ref = run_both(p, dims, nstep, sdg.FLAG_MIXED)
+    err_l2 = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err_l2 <= 1e-5, err_l2
+    assert rel_maxnorm(got, ref) <= 1e-4
+
+
+def test_minmax_and_diagnostics():
+    p = 5
+    ops, mesh, omesh, (q, u, v, w) = case(p, (3, 3, 3))
+    H = sdg.Handle(ops, mesh, 0)
+    H.set_state(q, u, v, w)
+    mn, mx = H.minmax()
+    assert mn == q[:, : mesh.Ne].min() and mx == q[:, : mesh.Ne].max()
+    W = sdg.lgl_weights(ops.x1D)
+    Wn = np.einsum("i,j,k->ijk", W, W, W).reshape(-1, order="F")
+    jac = (1 / 3) ** 3 / 8
+    mass, l2 = H.diagnostics(W, jac)
+    qe = q[:, : mesh.Ne]
+    assert abs(mass - np.sum(Wn[:, None] * jac * qe)) < 1e-13
+    assert abs(l2 - np.sqrt(np.sum(Wn[:, None] * jac * qe * qe))) < 1e-13
+    # mass is conserved by the scheme to rounding
+    dt = 0.1 * (1 / 3) / 36
+    H.rk3_steps(dt, 10)
+    mass2, _ = H.diagnostics(W, jac)
+    assert abs(mass2 - mass) < 1e-13
+    H.close()
+
+
+def test_device_pointer_entry():
+    import torch
+    p = 6
+    ops, mesh, omesh, (q, u, v, w) = case(p)
+    H = sdg.Handle(ops, mesh, sdg.FLAG_EXACT)
+    dev = [torch.from_numpy(a.reshape(-1, order="F")).cuda() for a in (q, u, v, w)]
+    out = torch.zeros_like(dev[0])
+    H.cal_tend_dev(out, *dev)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(mesh.Np, mesh.NeA, order="F")[:, : mesh.Ne]
+    ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+    assert np.array_equal(got, ref)
+    # update_halo on device == host update_halo
+    g = dev[0].clone()
+    g[mesh.Np * mesh.Ne:] = 0
+    H.update_halo_dev(g)
+    torch.cuda.synchronize()
+    assert np.array_equal(g.cpu().numpy(), q.reshape(-1, order="F"))
+    H.close()
+
+
+def test_full_size_rhs_against_oracle():
+    """32^3 elements, p = 7 (16.8 M DOF): one tendency vs the oracle."""
+    p = 7
+    ops = sdg.read_operators(p)
+    mesh = sdg.mesh_setup(32, 32, 32, p, ops.x1D)
+    q, u, v, w = sdg.init_fields(mesh, ic_kind=1, seed=1, vel_kind=0, vel=(1.0, 0.5, 0.25))
+    H = sdg.Handle(ops, mesh, 0)
+    got = H.cal_tend(q, u, v, w)[:, : mesh.Ne]
+    H.close()
+    omesh = orc.mesh_setup(32, 32, 32, p, ops.x1D)
+    ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+    assert rel_maxnorm(got, ref) <= TOL
