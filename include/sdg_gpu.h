@@ -197,6 +197,12 @@ int sdg_timers(sdg_handle* h, double* t4);
 /* Number of fused-kernel launches issued so far by the handle. */
 long long sdg_launch_count(sdg_handle* h);
 
+/* Selects the fused-kernel variant: 0 = automatic (default; also set by the
+ * environment variable SDG_KERNEL=block|pipe at sdg_init), 1 = one element
+ * tile per block, 2 = persistent blocks with a bulk-copy (TMA) ring.  Both
+ * compute identical results; the choice only affects speed. */
+int sdg_set_kernel_variant(sdg_handle* h, int variant);
+
 #ifdef __cplusplus
 }
 #endif

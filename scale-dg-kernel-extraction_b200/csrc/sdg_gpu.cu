@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -159,6 +160,10 @@ struct sdg_handle {
   int Nq = 0, Np = 0, NfpTot = 0, Ne = 0, NeA = 0, NhaloNode = 0;
   int flags = 0;
   bool direct_ok = false;
+  int variant = kVariantAuto;  // KernelVariant of the fused kernel
+  int num_sms = 148;
+  int* status = nullptr;       // device status word of bounded waits
+  bool primed = false;
   cudaStream_t stream = nullptr;
   std::vector<double> D;  // row-major D(i,l)
 
@@ -214,7 +219,7 @@ void free_handle(sdg_handle* h) {
                   h->io[1],  h->io[2],  h->io[3],   h->io[4],     h->q0,
                   h->qa,     h->qb,     h->vel[0],  h->vel[1],    h->vel[2],
                   h->vel64[0], h->vel64[1], h->vel64[2], h->red_partials,
-                  h->red_counter, h->red_result, h->lgl_wn};
+                  h->red_counter, h->red_result, h->lgl_wn, h->status};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -239,7 +244,24 @@ LaunchSpec base_spec(const sdg_handle* h, bool f32) {
   s.nelem = h->Ne;
   s.D = h->D.data();
   s.stream = h->stream;
+  s.variant = h->variant;
+  s.status = h->status;
+  s.num_sms = h->num_sms;
   return s;
+}
+
+// Reads and clears the device status word after the stream has drained.
+int check_status(sdg_handle* h) {
+  int st = 0;
+  cudaError_t e = cudaMemcpy(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess)
+    return fail(SDG_ERR_CUDA, "status read failed: %s", cudaGetErrorString(e));
+  if (st != 0) {
+    cudaMemset(h->status, 0, sizeof(int));
+    return fail(SDG_ERR_CUDA, "a fused kernel's bounded wait on its bulk copies timed out "
+                "(status %d); results of that launch are invalid", st);
+  }
+  return SDG_OK;
 }
 
 int launch_halo(sdg_handle* h, void* f, bool f32, cudaStream_t st) {
@@ -402,6 +424,29 @@ int enqueue_stage(sdg_handle* h, int st, double dt) {
   return launch_tend(s);
 }
 
+// Runs the one-time attribute/occupancy set-up of the three stage kernels
+// outside any stream capture.
+int prime_stages(sdg_handle* h) {
+  if (h->primed) return SDG_OK;
+  for (int st = 0; st < 3; ++st) {
+    LaunchSpec s = base_spec(h, mixed(h));
+    s.kind = mixed(h) ? (kStageMixed1 + st) : kStageF64;
+    s.q = st == 0 ? static_cast<const void*>(h->q0) : (st == 1 ? h->qa : h->qb);
+    s.u = h->vel[0];
+    s.v = h->vel[1];
+    s.w = h->vel[2];
+    s.q0 = h->q0;
+    s.out = h->qa;
+    s.pbase = h->direct_ok ? h->pb_direct : h->pb_halo;
+    s.rk_a = st == 0 ? 0.0 : 0.5;
+    s.nelem = 0;
+    int rc = launch_tend(s);
+    if (rc) return rc;
+  }
+  h->primed = true;
+  return SDG_OK;
+}
+
 // Enqueues one SSP-RK3 step (main.f90:51-74) on the handle's stream.
 int enqueue_step(sdg_handle* h, double dt) {
   for (int st = 0; st < 3; ++st) {
@@ -487,6 +532,14 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
                 "CPU path", cudaGetErrorString(ce));
   }
   cudaGetDevice(&h->dev);
+  {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, h->dev) == cudaSuccess)
+      h->num_sms = prop.multiProcessorCount;
+    const char* kv = std::getenv("SDG_KERNEL");
+    if (kv && std::strcmp(kv, "block") == 0) h->variant = kVariantBlock;
+    else if (kv && std::strcmp(kv, "pipe") == 0) h->variant = kVariantPipe;
+  }
 
   auto bail = [&](int code) { free_handle(h); return code; };
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -518,7 +571,9 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
       !(h->red_result = dev_alloc<double>(2, &rc)) ||
       !(h->lgl_wn = dev_alloc<double>(Np, &rc)))
     return bail(rc);
-  if (cudaMemset(h->red_counter, 0, sizeof(unsigned int)) != cudaSuccess)
+  if (!(h->status = dev_alloc<int>(1, &rc))) return bail(rc);
+  if (cudaMemset(h->red_counter, 0, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(SDG_ERR_CUDA, "cudaMemset failed"));
   *out = h;
   return SDG_OK;
@@ -576,6 +631,7 @@ int sdg_cal_tend(sdg_handle* h, double* dqdt, const double* q,
                            cudaMemcpyDeviceToHost, h->stream));
   SDG_CUDA(cudaEventRecord(h->ev1, h->stream));
   SDG_CUDA(cudaStreamSynchronize(h->stream));
+  if ((rc = check_status(h))) return rc;
   float a = 0, b = 0, c = 0;
   cudaEventElapsedTime(&a, h->ev0, e2);
   cudaEventElapsedTime(&b, e2, e3);
@@ -639,7 +695,7 @@ int sdg_get_field(sdg_handle* h, int which, double* host) {
   SDG_CUDA(cudaMemcpyAsync(host, src, NE * sizeof(double), cudaMemcpyDeviceToHost,
                            h->stream));
   SDG_CUDA(cudaStreamSynchronize(h->stream));
-  return SDG_OK;
+  return check_status(h);
 }
 
 int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps) {
@@ -649,6 +705,7 @@ int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps) {
   if (!h->have_q || !h->have_vel[0] || !h->have_vel[1] || !h->have_vel[2])
     return fail(SDG_ERR_STATE, "upload q, u, v and w with sdg_set_field first");
   if (nsteps == 0) return SDG_OK;
+  if ((rc = prime_stages(h))) return rc;
   if (!h->graph || h->graph_dt != dt) {
     if (h->graph) {
       cudaGraphExecDestroy(h->graph);
@@ -698,7 +755,7 @@ int sdg_synchronize(sdg_handle* h) {
   if (rc) return rc;
   SDG_CUDA(cudaStreamSynchronize(h->stream));
   account_rk(h);
-  return SDG_OK;
+  return check_status(h);
 }
 
 int sdg_minmax(sdg_handle* h, double* qmin, double* qmax) {
@@ -712,6 +769,7 @@ int sdg_minmax(sdg_handle* h, double* qmin, double* qmax) {
   double r[2];
   SDG_CUDA(cudaMemcpyAsync(r, h->red_result, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
   SDG_CUDA(cudaStreamSynchronize(h->stream));
+  if ((rc = check_status(h))) return rc;
   if (qmin) *qmin = r[0];
   if (qmax) *qmax = r[1];
   return SDG_OK;
@@ -763,5 +821,18 @@ int sdg_timers(sdg_handle* h, double* t4) {
 }
 
 long long sdg_launch_count(sdg_handle* h) { return h ? h->launches : -1; }
+
+int sdg_set_kernel_variant(sdg_handle* h, int variant) {
+  if (!h) return fail(SDG_ERR_ARG, "null handle");
+  if (variant < kVariantAuto || variant > kVariantPipe)
+    return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block) or 2 (pipelined)");
+  if (variant != h->variant && h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->variant = variant;
+  h->primed = false;
+  return SDG_OK;
+}
 
 }  // extern "C"

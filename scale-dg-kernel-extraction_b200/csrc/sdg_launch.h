@@ -41,7 +41,16 @@ struct LaunchSpec {
   double rk_a, rk_b, dt;
   const double* D;     // row-major D(i,l), NQ*NQ
   cudaStream_t stream;
+  int variant;         // KernelVariant
+  int* status;         // device status word (bounded-wait timeouts)
+  int num_sms;         // multiprocessors of the device
 };
+
+// Kernel variants: the one-tile-per-block kernel (tend_kernel) and the
+// persistent bulk-copy pipelined kernel (tend_pipe_kernel); identical
+// arithmetic.  Auto picks the pipelined one when two blocks fit per SM and
+// every array is 16-byte aligned.
+enum KernelVariant { kVariantAuto = 0, kVariantBlock = 1, kVariantPipe = 2 };
 
 // Returns 0 when launched, -1 when this unit does not hold spec.nq,
 // otherwise a cudaError_t value.

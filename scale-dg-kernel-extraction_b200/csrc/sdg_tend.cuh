@@ -191,6 +191,7 @@ struct TendArgs {
   int elem0;            // first element of this launch
   int nelem;            // elements in this launch
   double rk_a, rk_b, dt;
+  int* status;          // device status word: nonzero after a timed-out wait
 };
 
 // ---------------------------------------------------------------------------
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
   constexpr int RS = G::RS;
   constexpr int PS = G::PS;
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   TC* smem = reinterpret_cast<TC*>(smem_raw);
 
   const int s = threadIdx.x / NQ2;           // element slot in the block

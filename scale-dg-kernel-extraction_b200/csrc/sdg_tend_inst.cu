@@ -1,8 +1,13 @@
 // Instantiates the fused tendency kernel for one polynomial order.
 // Compiled once per NQ = p+1 (2..16) with -DSDG_NQ=<NQ>, so the fifteen
 // fully unrolled variants build in parallel.
+#include <stdint.h>
+
+#include <algorithm>
+
 #include "sdg_launch.h"
 #include "sdg_tend.cuh"
+#include "sdg_tend_pipe.cuh"
 
 #ifndef SDG_NQ
 #error "SDG_NQ must be defined"
@@ -34,14 +39,46 @@ int run(const LaunchSpec& s) {
   a.rk_a = s.rk_a;
   a.rk_b = s.rk_b;
   a.dt = s.dt;
+  a.status = s.status;
   DMat<NQ, TC> d;
   for (int i = 0; i < NQ * NQ; ++i) d.d[i] = static_cast<TC>(s.D[i]);
+  using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
+  auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  const bool can_pipe = P::BYTES <= 110 * 1024 && aligned(s.q) && aligned(s.u) &&
+                        aligned(s.v) && aligned(s.w) && (!STAGE || aligned(s.q0));
+  const bool pipe = s.variant == kVariantPipe ? can_pipe
+                    : s.variant == kVariantBlock ? false
+                                                 : can_pipe;
+  if (pipe) {
+    // Attribute and occupancy set-up runs on the first call (a call with
+    // nelem == 0 only primes it, e.g. before a stream capture).
+    auto kern = tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
+    static int blocks_per_sm = 0;  // per instantiation; the plan is fixed
+    if (blocks_per_sm == 0) {
+      cudaError_t e = cudaFuncSetAttribute(
+          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(P::BYTES));
+      if (e != cudaSuccess) return static_cast<int>(e);
+      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      int nb = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::THREADS, P::BYTES);
+      if (e != cudaSuccess) return static_cast<int>(e);
+      blocks_per_sm = nb > 0 ? nb : 1;
+    }
+    if (s.nelem <= 0) return 0;
+    const int ntiles = (s.nelem + G::EPB - 1) / G::EPB;
+    const int grid = std::min(ntiles, blocks_per_sm * (s.num_sms > 0 ? s.num_sms : 148));
+    kern<<<grid, G::THREADS, P::BYTES, s.stream>>>(a, d);
+    return static_cast<int>(cudaGetLastError());
+  }
+
   auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
   const size_t smem = SmemLayout<NQ, TC>::BYTES;
-  if (smem > 48 * 1024) {
+  static bool attr_done = false;  // per instantiation
+  if (smem > 48 * 1024 && !attr_done) {
     cudaError_t e = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return static_cast<int>(e);
+    attr_done = true;
   }
   if (s.nelem <= 0) return 0;
   const int blocks = (s.nelem + G::EPB - 1) / G::EPB;

@@ -44,6 +44,8 @@ FLAG_MIXED = 4
 
 FIELD_Q, FIELD_U, FIELD_V, FIELD_W = 0, 1, 2, 3
 
+VARIANT_AUTO, VARIANT_BLOCK, VARIANT_PIPE = 0, 1, 2
+
 # Exported symbols and their signatures (must match include/sdg_gpu.h).
 _I, _D, _P, _LL = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
 _U64 = ctypes.c_ulonglong
@@ -74,6 +76,7 @@ SIGNATURES = {
     "sdg_field_dev_ptr": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "sdg_timers": (_I, [_P, _P]),
     "sdg_launch_count": (_LL, [_P]),
+    "sdg_set_kernel_variant": (_I, [_P, _I]),
 }
 
 
@@ -264,7 +267,9 @@ class Handle:
         _check(lib().sdg_update_halo_dev(self._h, f.data_ptr(), stream))
 
     def set_field(self, which, host):
-        host = _f64(host)
+        if not (isinstance(host, np.ndarray) and host.dtype == np.float64 and
+                (host.flags.c_contiguous or host.flags.f_contiguous)):
+            host = _f64(host)
         if host.size < self.mesh.Np * self.mesh.Ne:
             raise SdgError(SDG_ERR_ARG, "field smaller than (Np, Ne)")
         _check(lib().sdg_set_field(self._h, which, _p(host)))
@@ -273,8 +278,14 @@ class Handle:
         for which, a in zip((FIELD_Q, FIELD_U, FIELD_V, FIELD_W), (q, u, v, w)):
             self.set_field(which, a)
 
-    def get_field(self, which=FIELD_Q):
-        out = np.zeros((self.mesh.Np, self.mesh.Ne), order="F")
+    def get_field(self, which=FIELD_Q, out=None):
+        """Field (Np, Ne) into `out` (any contiguous float64 array of that
+        size, e.g. a pinned buffer) or a new array."""
+        if out is None:
+            out = np.zeros((self.mesh.Np, self.mesh.Ne), order="F")
+        elif out.dtype != np.float64 or out.size < self.mesh.Np * self.mesh.Ne or not (
+                out.flags.c_contiguous or out.flags.f_contiguous):
+            raise SdgError(SDG_ERR_ARG, "get_field: bad output array")
         _check(lib().sdg_get_field(self._h, which, _p(out)))
         return out
 
@@ -318,6 +329,10 @@ class Handle:
 
     def launch_count(self):
         return int(lib().sdg_launch_count(self._h))
+
+    def set_kernel_variant(self, variant):
+        """0 automatic, 1 one tile per block, 2 persistent bulk-copy ring."""
+        _check(lib().sdg_set_kernel_variant(self._h, variant))
 
 
 # ---------------------------------------------------------------------------

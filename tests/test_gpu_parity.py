@@ -188,3 +188,52 @@ def test_full_size_rhs_against_oracle():
     omesh = orc.mesh_setup(32, 32, 32, p, ops.x1D)
     ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
     assert rel_maxnorm(got, ref) <= TOL
+
+
+@pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE])
+@pytest.mark.parametrize("p", range(1, 16))
+def test_kernel_variants_bitwise(p, variant):
+    """Both kernel variants (one tile per block; persistent bulk-copy ring)
+    reproduce the oracle bit for bit in exact mode, tendency and RK stages."""
+    ops, mesh, omesh, (q, u, v, w) = case(p, (3, 2, 3) if p <= 7 else (2, 2, 3))
+    h = sdg.Handle(ops, mesh, sdg.FLAG_EXACT)
+    h.set_kernel_variant(variant)
+    got = h.cal_tend(q, u, v, w)[:, : mesh.Ne]
+    ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+    assert np.array_equal(got, ref)
+    dt = 0.1 / 3 / (p + 1) ** 2
+    h.set_state(q, u, v, w)
+    h.rk3_steps(dt, 3)
+    got = h.get_field()
+    qo = q.copy(order="F")
+    orc.run_rk3(orc.OPT1, qo, u, v, w, ops, omesh, dt, 3)
+    assert np.array_equal(got, qo[:, : mesh.Ne])
+    h.close()
+
+
+@pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE])
+def test_mixed_variants_agree(variant):
+    p, dims, nstep = 7, (4, 3, 5), 10
+    ops, mesh, omesh, (q, u, v, w) = case(p, dims)
+    dt = 0.1 / 5 / 64
+    res = []
+    for var in (sdg.VARIANT_BLOCK, variant):
+        h = sdg.Handle(ops, mesh, sdg.FLAG_MIXED)
+        h.set_kernel_variant(var)
+        h.set_state(q, u, v, w)
+        h.rk3_steps(dt, nstep)
+        res.append(h.get_field())
+        h.close()
+    assert np.array_equal(res[0], res[1])
+
+
+def test_partial_last_tile_and_uneven_sizes():
+    """Element counts that leave a partial last tile (pipelined variant)."""
+    for p, dims in ((2, (5, 3, 1)), (4, (3, 1, 3)), (6, (1, 3, 3)), (7, (3, 3, 1))):
+        ops, mesh, omesh, (q, u, v, w) = case(p, dims)
+        h = sdg.Handle(ops, mesh, sdg.FLAG_EXACT)
+        h.set_kernel_variant(sdg.VARIANT_PIPE)
+        got = h.cal_tend(q, u, v, w)[:, : mesh.Ne]
+        ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
+        assert np.array_equal(got, ref), (p, dims)
+        h.close()
