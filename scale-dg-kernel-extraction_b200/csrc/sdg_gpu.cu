@@ -539,6 +539,7 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
     const char* kv = std::getenv("SDG_KERNEL");
     if (kv && std::strcmp(kv, "block") == 0) h->variant = kVariantBlock;
     else if (kv && std::strcmp(kv, "pipe") == 0) h->variant = kVariantPipe;
+    else if (kv && std::strcmp(kv, "blockocc") == 0) h->variant = kVariantBlockOcc;
   }
 
   auto bail = [&](int code) { free_handle(h); return code; };
@@ -824,8 +825,9 @@ long long sdg_launch_count(sdg_handle* h) { return h ? h->launches : -1; }
 
 int sdg_set_kernel_variant(sdg_handle* h, int variant) {
   if (!h) return fail(SDG_ERR_ARG, "null handle");
-  if (variant < kVariantAuto || variant > kVariantPipe)
-    return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block) or 2 (pipelined)");
+  if (variant < kVariantAuto || variant > kVariantBlockOcc)
+    return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block), 2 (pipelined) "
+                "or 3 (block, 8 blocks per SM)");
   if (variant != h->variant && h->graph) {
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;

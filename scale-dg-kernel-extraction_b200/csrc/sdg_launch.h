@@ -50,7 +50,14 @@ struct LaunchSpec {
 // persistent bulk-copy pipelined kernel (tend_pipe_kernel); identical
 // arithmetic.  Auto picks the pipelined one when two blocks fit per SM and
 // every array is 16-byte aligned.
-enum KernelVariant { kVariantAuto = 0, kVariantBlock = 1, kVariantPipe = 2 };
+// kVariantBlockOcc is the one-tile-per-block kernel built for eight resident
+// blocks per SM (p = 3..7; other orders use kVariantBlock).
+enum KernelVariant {
+  kVariantAuto = 0,
+  kVariantBlock = 1,
+  kVariantPipe = 2,
+  kVariantBlockOcc = 3
+};
 
 // Returns 0 when launched, -1 when this unit does not hold spec.nq,
 // otherwise a cudaError_t value.

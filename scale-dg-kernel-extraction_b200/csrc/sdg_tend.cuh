@@ -67,11 +67,14 @@ struct Ar<double, true> {
     return __dadd_rn(t, __dmul_rn(a, b));
   }
 };
+// The fast policies fuse exactly where `mad` is written and nowhere else
+// (the _rn intrinsics keep the compiler from contracting on its own), so
+// every kernel variant computes bit-identical results.
 template <>
 struct Ar<double, false> {
-  static __device__ __forceinline__ double mul(double a, double b) { return a * b; }
-  static __device__ __forceinline__ double add(double a, double b) { return a + b; }
-  static __device__ __forceinline__ double sub(double a, double b) { return a - b; }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
   static __device__ __forceinline__ double mad(double a, double b, double t) { return fma(a, b, t); }
 };
 template <>
@@ -85,9 +88,9 @@ struct Ar<float, true> {
 };
 template <>
 struct Ar<float, false> {
-  static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
-  static __device__ __forceinline__ float add(float a, float b) { return a + b; }
-  static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
   static __device__ __forceinline__ float mad(float a, float b, float t) { return fmaf(a, b, t); }
 };
 
@@ -197,9 +200,11 @@ struct TendArgs {
 // ---------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------
+// MINB is the minimum number of resident blocks per SM the build must allow
+// (it caps registers per thread); 1 leaves the compiler free.
 template <int NQ, typename TQ, typename TV, typename TO, typename TC,
-          bool EXACT, int ORDER, bool STAGE>
-__global__ void __launch_bounds__(Geo<NQ>::THREADS)
+          bool EXACT, int ORDER, bool STAGE, int MINB = 1>
+__global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
     tend_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
                 const __grid_constant__ DMat<NQ, TC> D) {
   using G = Geo<NQ>;
@@ -358,8 +363,8 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
       double qd;
       if constexpr (sizeof(TQ) == sizeof(TC)) qd = static_cast<double>(qc[k]);
       else qd = static_cast<double>(A.q[n]);
-      double r = AD::mul(A.rk_b, AD::add(qd, AD::mul(A.dt, static_cast<double>(dqdt))));
-      if (A.rk_a != 0.0) r = AD::add(AD::mul(A.rk_a, A.q0[n]), r);
+      double r = AD::mul(A.rk_b, AD::mad(A.dt, static_cast<double>(dqdt), qd));
+      if (A.rk_a != 0.0) r = AD::mad(A.rk_a, A.q0[n], r);
       A.out[n] = static_cast<TO>(r);
     }
   }

@@ -46,9 +46,7 @@ int run(const LaunchSpec& s) {
   auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
   const bool can_pipe = P::BYTES <= 110 * 1024 && aligned(s.q) && aligned(s.u) &&
                         aligned(s.v) && aligned(s.w) && (!STAGE || aligned(s.q0));
-  const bool pipe = s.variant == kVariantPipe ? can_pipe
-                    : s.variant == kVariantBlock ? false
-                                                 : can_pipe;
+  const bool pipe = (s.variant == kVariantPipe || s.variant == kVariantAuto) && can_pipe;
   if (pipe) {
     // Attribute and occupancy set-up runs on the first call (a call with
     // nelem == 0 only primes it, e.g. before a stream capture).
@@ -71,8 +69,24 @@ int run(const LaunchSpec& s) {
     return static_cast<int>(cudaGetLastError());
   }
 
-  auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
   const size_t smem = SmemLayout<NQ, TC>::BYTES;
+  if constexpr (NQ >= 4 && NQ <= 8) {
+    // One tile per block, built for 8 resident 128-thread blocks per SM
+    // (64 registers per thread) with the largest shared-memory carveout.
+    if (s.variant == kVariantBlockOcc) {
+      auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, 8>;
+      static bool carve_done = false;
+      if (!carve_done) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        carve_done = true;
+      }
+      if (s.nelem <= 0) return 0;
+      const int blocks = (s.nelem + G::EPB - 1) / G::EPB;
+      kern<<<blocks, G::THREADS, smem, s.stream>>>(a, d);
+      return static_cast<int>(cudaGetLastError());
+    }
+  }
+  auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
   static bool attr_done = false;  // per instantiation
   if (smem > 48 * 1024 && !attr_done) {
     cudaError_t e = cudaFuncSetAttribute(

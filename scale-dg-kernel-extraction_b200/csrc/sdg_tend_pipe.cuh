@@ -346,8 +346,8 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
           double qd;
           if constexpr (sizeof(TQ) == sizeof(TC)) qd = static_cast<double>(qc[k]);
           else qd = qs[k];
-          double r = AD::mul(A.rk_b, AD::add(qd, AD::mul(A.dt, static_cast<double>(dqdt))));
-          if (A.rk_a != 0.0) r = AD::add(AD::mul(A.rk_a, q0v[k]), r);
+          double r = AD::mul(A.rk_b, AD::mad(A.dt, static_cast<double>(dqdt), qd));
+          if (A.rk_a != 0.0) r = AD::mad(A.rk_a, q0v[k], r);
           A.out[n] = static_cast<TO>(r);
         }
       }
