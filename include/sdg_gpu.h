@@ -203,6 +203,20 @@ long long sdg_launch_count(sdg_handle* h);
  * compute identical results; the choice only affects speed. */
 int sdg_set_kernel_variant(sdg_handle* h, int variant);
 
+/* min and max of n doubles at device pointer q, written to the device
+ * pointer out2 (out2[0] = min, out2[1] = max), asynchronously on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream).  No counterpart in the
+ * reference: this is sdg_minmax's reduction for callers that cannot
+ * allocate device memory (a time loop under a fixed device-memory budget,
+ * or a caller with a raw device array and no handle).  It allocates
+ * nothing: its scratch is a fixed 64 KB file-scope device array that every
+ * GPU loading the library holds until exit, so n may be at most 33,554,432
+ * (larger n returns SDG_ERR_ARG).  All calls share that scratch: calls that
+ * overlap on the GPU race, so serialise them.  The first call on a device
+ * looks up the scratch's address; make it before any stream capture. */
+int sdg_minmax_dev_noalloc(const double* q, long long n, double* out2,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,7 @@ SIGNATURES = {
     "sdg_timers": (_I, [_P, _P]),
     "sdg_launch_count": (_LL, [_P]),
     "sdg_set_kernel_variant": (_I, [_P, _I]),
+    "sdg_minmax_dev_noalloc": (_I, [_P, _LL, _P, _P]),
 }
 
 
