@@ -203,6 +203,88 @@ long long sdg_launch_count(sdg_handle* h);
  * compute identical results; the choice only affects speed. */
 int sdg_set_kernel_variant(sdg_handle* h, int variant);
 
+/* ---------------------------------------------------------------------
+ * Batched ensembles: many independent periodic-box instances of uneven
+ * size and order advanced together (the reference runs one mesh per
+ * process, main.f90:51-80; this is its ensemble form).
+ * --------------------------------------------------------------------- */
+typedef struct sdg_batch sdg_batch;
+
+/* flags: 0 (FMA FP64), SDG_FLAG_EXACT (+ SDG_FLAG_ORDER_GENERAL), or
+ * SDG_FLAG_MIXED.  Errors with SDG_ERR_CUDA when no device exists. */
+int sdg_batch_create(sdg_batch** b, int flags);
+
+/* Adds a periodic unit box of NeX x NeY x NeZ elements of order p with its
+ * operators (D1D, Lift_mat as read by sdg_read_operators; every instance of
+ * one order must pass the same operators), initial state q and velocity
+ * u, v, w (host arrays of at least Np*Ne values, (Np, Ne) layout) and time
+ * step dt.  The mesh tables are those of sdg_mesh_setup on that box.
+ * Returns the instance id in *id. */
+int sdg_batch_add(sdg_batch* b, int NeX, int NeY, int NeZ, int p,
+                  const double* D1D, const double* Lift_mat, const double* q,
+                  const double* u, const double* v, const double* w, double dt,
+                  int* id);
+
+/* Freezes membership.  Instances of one order form a group whose RK stage
+ * is one persistent launch over a tile table; with autotune != 0 each
+ * group's tile shape (kernel variant: elements per block x nodes per
+ * thread) is chosen by timing the candidates on the group's instances.
+ * One RK step of all groups is captured as a CUDA graph. */
+int sdg_batch_commit(sdg_batch* b, int autotune);
+
+/* Advances every instance by nsteps SSP-RK3 steps (graph replays);
+ * synchronous. */
+int sdg_batch_run(sdg_batch* b, int nsteps);
+
+/* Copies instance `id`'s state q (Np, Ne) to the host. */
+int sdg_batch_get(sdg_batch* b, int id, double* q);
+
+/* Up to n values: instances, total DOF, run seconds, DOF x steps run,
+ * groups, then per group p, mixed, tiles, chosen variant and the tuned
+ * stage times (ms) of the pipelined, block and 8-blocks-per-SM variants.
+ * Returns the number of values available. */
+int sdg_batch_info(sdg_batch* b, double* out, int n);
+
+int sdg_batch_destroy(sdg_batch* b);
+
+/* ---------------------------------------------------------------------
+ * Serving loop: solve requests admitted as device memory frees up, all
+ * admitted requests advanced together one RK step at a time.
+ * --------------------------------------------------------------------- */
+typedef struct sdg_server sdg_server;
+
+/* Starts a server whose requests may use at most max_bytes of device memory
+ * (<= 0: 85% of the memory free now).  A worker thread drives the GPU. */
+int sdg_serve_create(sdg_server** s, double max_bytes);
+
+/* Queues a request: the box, operators and host arrays as sdg_batch_add,
+ * nsteps RK3 steps, flags 0 (FMA FP64) or SDG_FLAG_MIXED.  The arrays are
+ * copied; the call returns at once with the request id.  A request larger
+ * than the server's memory cap is rejected with SDG_ERR_ARG. */
+int sdg_serve_submit(sdg_server* s, int NeX, int NeY, int NeZ, int p,
+                     const double* D1D, const double* Lift_mat, const double* q,
+                     const double* u, const double* v, const double* w,
+                     double dt, int nsteps, int flags, int* id);
+
+/* State of a request: 0 queued, 1 running, 2 done, 3 failed.  times[0] =
+ * queue wait (s, -1 until admitted), times[1] = time to solution (s, -1
+ * until done). */
+int sdg_serve_poll(sdg_server* s, int id, int* state, double* times2);
+
+/* Copies a done request's final q (Np, Ne) to the host and forgets it. */
+int sdg_serve_result(sdg_server* s, int id, double* q);
+
+/* Blocks until no request is queued or running (timeout_s <= 0: no
+ * limit); reports the first request failure, if any. */
+int sdg_serve_wait(sdg_server* s, double timeout_s);
+
+/* out4: device-busy seconds, DOF x RK steps done, RK iterations run, device
+ * bytes held by admitted requests. */
+int sdg_serve_stats(sdg_server* s, double* out4);
+
+/* Stops the worker and frees everything. */
+int sdg_serve_destroy(sdg_server* s);
+
 /* min and max of n doubles at device pointer q, written to the device
  * pointer out2 (out2[0] = min, out2[1] = max), asynchronously on `stream`
  * (a cudaStream_t; NULL = the legacy default stream).  No counterpart in the

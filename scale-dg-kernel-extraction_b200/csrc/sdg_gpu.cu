@@ -18,15 +18,29 @@
 #include "sdg_launch.h"
 
 namespace sdg {
-namespace {
 
-#define SDG_CUDA(call)                                                     \
-  do {                                                                     \
-    cudaError_t err_ = (call);                                             \
-    if (err_ != cudaSuccess)                                               \
-      return fail(SDG_ERR_CUDA, "%s failed: %s", #call,                    \
-                  cudaGetErrorString(err_));                               \
-  } while (0)
+int pipe_info(int nq, int kind, int* epb) {
+  typedef int (*Fn)(int, int*);
+  static const Fn table[17] = {nullptr,       nullptr,       pipe_info_nq2,  pipe_info_nq3,
+                               pipe_info_nq4, pipe_info_nq5, pipe_info_nq6,  pipe_info_nq7,
+                               pipe_info_nq8, pipe_info_nq9, pipe_info_nq10, pipe_info_nq11,
+                               pipe_info_nq12, pipe_info_nq13, pipe_info_nq14, pipe_info_nq15,
+                               pipe_info_nq16};
+  *epb = 1;
+  if (nq < 2 || nq > 16) return 0;
+  return table[nq](kind, epb);
+}
+
+int pipe_elems_per_tile(int nq) {
+  int epb = 1;
+  pipe_info(nq, kTendF64, &epb);
+  return epb;
+}
+
+bool pipe_supported(int nq, int kind) {
+  int epb = 1;
+  return pipe_info(nq, kind, &epb) != 0;
+}
 
 int launch_tend(const LaunchSpec& s) {
   typedef int (*Fn)(const LaunchSpec&);
@@ -43,6 +57,16 @@ int launch_tend(const LaunchSpec& s) {
                 cudaGetErrorString(static_cast<cudaError_t>(rc)));
   return SDG_OK;
 }
+
+namespace {
+
+#define SDG_CUDA(call)                                                     \
+  do {                                                                     \
+    cudaError_t err_ = (call);                                             \
+    if (err_ != cudaSuccess)                                               \
+      return fail(SDG_ERR_CUDA, "%s failed: %s", #call,                    \
+                  cudaGetErrorString(err_));                               \
+  } while (0)
 
 // ---------------------------------------------------------------------------
 // Auxiliary kernels

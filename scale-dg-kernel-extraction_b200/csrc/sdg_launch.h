@@ -44,7 +44,24 @@ struct LaunchSpec {
   int variant;         // KernelVariant
   int* status;         // device status word (bounded-wait timeouts)
   int num_sms;         // multiprocessors of the device
+  // Batched launch (pipelined kernel only): device arrays of BatchInst and
+  // BatchTile (sdg_tend.cuh) and the tile count; null for one instance.
+  const void* batch_insts;
+  const void* batch_tiles;
+  int batch_ntiles;
 };
+
+// Elements per tile of the pipelined kernel for a given order (the tile
+// size a batch's tile table must use).
+int pipe_elems_per_tile(int nq);
+
+// Whether the pipelined kernel can run kind `kind` at this order (its
+// shared-memory plan fits).
+bool pipe_supported(int nq, int kind);
+
+// Launches the fused kernel described by `s`; returns SDG_OK or an SDG_ERR_*
+// status with the thread's last error set.
+int launch_tend(const LaunchSpec& s);
 
 // Kernel variants: the one-tile-per-block kernel (tend_kernel) and the
 // persistent bulk-copy pipelined kernel (tend_pipe_kernel); identical
@@ -76,6 +93,24 @@ int launch_tend_nq13(const LaunchSpec&);
 int launch_tend_nq14(const LaunchSpec&);
 int launch_tend_nq15(const LaunchSpec&);
 int launch_tend_nq16(const LaunchSpec&);
+
+// Per order: elements per tile of the pipelined kernel (*epb) and whether
+// its shared-memory plan fits for `kind` (return value).
+int pipe_info_nq2(int kind, int* epb);
+int pipe_info_nq3(int kind, int* epb);
+int pipe_info_nq4(int kind, int* epb);
+int pipe_info_nq5(int kind, int* epb);
+int pipe_info_nq6(int kind, int* epb);
+int pipe_info_nq7(int kind, int* epb);
+int pipe_info_nq8(int kind, int* epb);
+int pipe_info_nq9(int kind, int* epb);
+int pipe_info_nq10(int kind, int* epb);
+int pipe_info_nq11(int kind, int* epb);
+int pipe_info_nq12(int kind, int* epb);
+int pipe_info_nq13(int kind, int* epb);
+int pipe_info_nq14(int kind, int* epb);
+int pipe_info_nq15(int kind, int* epb);
+int pipe_info_nq16(int kind, int* epb);
 
 // Shared-memory bytes and threads per block of the fused kernel.
 void tend_block_shape(int nq, bool fp32, int* threads, size_t* smem,

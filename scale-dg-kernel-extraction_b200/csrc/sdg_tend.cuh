@@ -195,6 +195,36 @@ struct TendArgs {
   int nelem;            // elements in this launch
   double rk_a, rk_b, dt;
   int* status;          // device status word: nonzero after a timed-out wait
+  // Batched launches (pipelined kernel only): per-instance arrays and a
+  // table of element tiles.  Null for a single instance, whose tiles are
+  // the consecutive elements elem0 .. elem0+nelem-1 of the arrays above.
+  const struct BatchInst* insts;
+  const struct BatchTile* tiles;
+  int ntiles;
+};
+
+// One ensemble instance of a batched launch.  Arrays have the single
+// instance's layout; q, u, v, w and q0 hold at least Np*Ne elements plus 16
+// bytes of slack (the bulk copies read whole 16-byte words).
+struct BatchInst {
+  const void* q;
+  const void* u;
+  const void* v;
+  const void* w;
+  const double* q0;
+  void* out;
+  const int* pbase;
+  const void* escale;
+  const void* fscale;
+  double dt;
+};
+
+// A tile: up to EPB consecutive elements e0 .. e0+n-1 of instance `inst`.
+struct BatchTile {
+  int inst;
+  int e0;
+  int n;
+  int pad;
 };
 
 // ---------------------------------------------------------------------------

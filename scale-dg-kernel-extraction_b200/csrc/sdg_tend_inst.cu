@@ -40,13 +40,21 @@ int run(const LaunchSpec& s) {
   a.rk_b = s.rk_b;
   a.dt = s.dt;
   a.status = s.status;
+  a.insts = static_cast<const BatchInst*>(s.batch_insts);
+  a.tiles = static_cast<const BatchTile*>(s.batch_tiles);
+  a.ntiles = s.batch_ntiles;
   DMat<NQ, TC> d;
   for (int i = 0; i < NQ * NQ; ++i) d.d[i] = static_cast<TC>(s.D[i]);
   using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
   auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-  const bool can_pipe = P::BYTES <= 110 * 1024 && aligned(s.q) && aligned(s.u) &&
-                        aligned(s.v) && aligned(s.w) && (!STAGE || aligned(s.q0));
-  const bool pipe = (s.variant == kVariantPipe || s.variant == kVariantAuto) && can_pipe;
+  const bool batch = s.batch_tiles != nullptr;
+  // Batched arrays are allocated 256-byte aligned by the batch itself.
+  const bool can_pipe = P::BYTES <= kPipeMaxSmem &&
+                        (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
+                                   aligned(s.w) && (!STAGE || aligned(s.q0))));
+  if (batch && !can_pipe) return static_cast<int>(cudaErrorNotSupported);
+  const bool pipe =
+      batch || ((s.variant == kVariantPipe || s.variant == kVariantAuto) && can_pipe);
   if (pipe) {
     // Attribute and occupancy set-up runs on the first call (a call with
     // nelem == 0 only primes it, e.g. before a stream capture).
@@ -58,14 +66,16 @@ int run(const LaunchSpec& s) {
       if (e != cudaSuccess) return static_cast<int>(e);
       cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       int nb = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::THREADS, P::BYTES);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, PipeGeo<NQ>::THREADS,
+                                                        P::BYTES);
       if (e != cudaSuccess) return static_cast<int>(e);
       blocks_per_sm = nb > 0 ? nb : 1;
     }
-    if (s.nelem <= 0) return 0;
-    const int ntiles = (s.nelem + G::EPB - 1) / G::EPB;
+    const int ntiles =
+        batch ? s.batch_ntiles : (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
+    if (ntiles <= 0) return 0;
     const int grid = std::min(ntiles, blocks_per_sm * (s.num_sms > 0 ? s.num_sms : 148));
-    kern<<<grid, G::THREADS, P::BYTES, s.stream>>>(a, d);
+    kern<<<grid, PipeGeo<NQ>::THREADS, P::BYTES, s.stream>>>(a, d);
     return static_cast<int>(cudaGetLastError());
   }
 
@@ -104,6 +114,25 @@ int run(const LaunchSpec& s) {
 
 #define SDG_CAT2(a, b) a##b
 #define SDG_CAT(a, b) SDG_CAT2(a, b)
+
+template <typename TQ, typename TV, typename TC, bool STAGE>
+constexpr bool pipe_fits() {
+  return PipePlan<NQ, TQ, TV, TC, STAGE>::BYTES <= kPipeMaxSmem;
+}
+
+// Pipelined-kernel facts for this order: elements per tile, and whether the
+// shared-memory plan of each kind fits.
+int SDG_CAT(pipe_info_nq, SDG_NQ)(int kind, int* epb) {
+  *epb = PipeGeo<NQ>::EPB;
+  switch (kind) {
+    case kTendF64: return pipe_fits<double, double, double, false>();
+    case kStageF64: return pipe_fits<double, double, double, true>();
+    case kStageMixed1: return pipe_fits<double, float, float, true>();
+    case kStageMixed2: return pipe_fits<float, float, float, true>();
+    case kStageMixed3: return pipe_fits<float, float, float, true>();
+    default: return 0;
+  }
+}
 
 int SDG_CAT(launch_tend_nq, SDG_NQ)(const LaunchSpec& s) {
   if (s.nq != NQ) return -1;

@@ -2,16 +2,28 @@
 // kernel (same arithmetic as tend_kernel in sdg_tend.cuh, same results).
 //
 // Each block loops over tiles of EPB consecutive elements.  The element data
-// a tile needs (q, u, v, w and, for RK stages, q0) are contiguous in HBM, so
-// one elected thread moves them into a shared-memory ring of NSTAGE tiles
-// with cp.async.bulk (the TMA bulk-copy engine), completing on an mbarrier
-// per ring slot; the copy of tile i+NSTAGE is issued as soon as tile i has
-// been read out of its slot.  Compute threads never stall on their own
-// loads: the bytes in flight per SM are set by the ring, not by occupancy.
-// The plus-side face values, which live in neighbouring elements, are
-// gathered with ordinary loads issued before the ring wait so that their
-// L2 latency overlaps it.  For p <= 7 each column thread keeps its 6*NQ
-// lift coefficients in registers for the whole persistent loop.
+// a tile needs (q, u, v, w) are contiguous in HBM, so one elected thread moves
+// them into a shared-memory ring of NSTAGE tiles with cp.async.bulk (the TMA
+// bulk-copy engine), completing on an mbarrier per ring slot; the copy of
+// tile i+NSTAGE is issued as soon as tile i has been read out of its slot.
+// Compute threads never stall on their own element loads: the bytes in
+// flight per SM are set by the ring, not by occupancy.  The plus-side face
+// values (in neighbouring elements) and the RK base state q0 are loaded with
+// ordinary loads issued before the ring wait, so their latency overlaps it.
+//
+// Thread mapping.  Column (a,b) of an element (its z-line) is owned by H
+// threads.  With H = 2 (Nq^2 a multiple of 32, i.e. p = 7 and p = 15) the two
+// owners sit in different warps, so the half index h is warp-uniform:
+//   h = 0: nodes k < Nq/2, the x-line (j,k) = (a,b), faces 1-2 at node
+//          (a,b), the -z face;
+//   h = 1: nodes k >= Nq/2, the y-line (i,k) = (a,b), faces 3-4, the +z face.
+// The two halves of a z-column meet in shared memory for the z-derivative.
+// With H = 1 one thread plays every role, as in tend_kernel.  Splitting
+// halves the registers per thread and doubles the warps per SM for the same
+// shared memory; each output's summation chain is unchanged.
+//
+// For p <= 7 each thread keeps the lift coefficients of its column nodes in
+// registers for the whole persistent loop.
 //
 // Every wait is bounded.  A wait that runs out sets *status and the block
 // drains its own copies (again bounded) and returns; the host reports the
@@ -25,6 +37,9 @@ namespace sdg {
 
 constexpr int kStatusWaitTimeout = 1;
 constexpr unsigned kWaitSpins = 1u << 22;
+// Largest shared-memory plan the pipelined kernel is used with: two blocks
+// of it fit on one SM (228 KB).
+constexpr size_t kPipeMaxSmem = 110 * 1024;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -76,10 +91,40 @@ __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Thread geometry of the pipelined kernel.
+// kSplitColumns enables the two-owners-per-column mapping (H = 2) where
+// Nq^2 is a multiple of 32.  Measured on B200 at p = 7 it doubles the warps
+// per SM but is slower (60.9 vs 70.6 G DOF-updates/s FP64): the kernel is
+// limited by the shared-memory pipe, and the split adds 15% wavefronts and
+// barrier stalls.  Kept for experiments; off by default.
+#ifndef SDG_SPLIT_COLUMNS
+#define SDG_SPLIT_COLUMNS 0
+#endif
+constexpr bool kSplitColumns = SDG_SPLIT_COLUMNS != 0;
+
+template <int NQ>
+struct PipeGeo {
+  static constexpr int NQ2 = NQ * NQ;
+  static constexpr int NP = NQ2 * NQ;
+  static constexpr int H = (kSplitColumns && NQ2 % 32 == 0) ? 2 : 1;  // owners per column
+  static constexpr int KH = NQ / H;                  // column nodes per thread
+  static constexpr int TPE = H * NQ2;                // threads per element
+  static constexpr int TARGET = (H == 2) ? 256 : 128;
+  static constexpr int EPB = TPE >= TARGET ? 1 : TARGET / TPE;
+  static constexpr int THREADS = EPB * TPE;
+  static constexpr int RS = Geo<NQ>::RS;
+  static constexpr int PS = Geo<NQ>::PS;
+  static constexpr int SBUF = Geo<NQ>::SBUF;
+  // Per-element work area: x- and y-line buffers, the four x/y faces'
+  // (q_minus, un_minus) pairs (the flux overwrites q_minus), the two z-face
+  // fluxes and, when H = 2, the z-column exchange buffer.
+  static constexpr int WORK_ELEM = 2 * SBUF + 8 * NQ2 + 2 * NQ2 + (H == 2 ? NP : 0);
+};
+
 // Shared-memory plan of the pipelined kernel.
 template <int NQ, typename TQ, typename TV, typename TC, bool STAGE>
 struct PipePlan {
-  using G = Geo<NQ>;
+  using G = PipeGeo<NQ>;
   static constexpr int EPB = G::EPB;
   static constexpr int NP = G::NP;
   static constexpr int NSTAGE = 2;
@@ -89,51 +134,181 @@ struct PipePlan {
   // each for 4- and 8-byte elements).
   static constexpr size_t QB = r16(sizeof(TQ) * EPB * NP + 32);
   static constexpr size_t VB = r16(sizeof(TV) * EPB * NP + 32);
-  static constexpr size_t Q0B = STAGE ? r16(sizeof(double) * EPB * NP + 32) : 0;
-  static constexpr size_t SLOT = QB + 3 * VB + Q0B;
-  static constexpr size_t WORK = r16(sizeof(TC) * SmemLayout<NQ, TC>::PER_ELEM * EPB);
+  static constexpr size_t SLOT = QB + 3 * VB;
+  static constexpr size_t WORK = r16(sizeof(TC) * G::WORK_ELEM * EPB);
   static constexpr size_t BARS = 16 * NSTAGE;
   static constexpr size_t BYTES = NSTAGE * SLOT + WORK + BARS;
   // Lift coefficients kept in registers when the column is short.
   static constexpr bool LIFT_REGS = NQ <= 8;
 };
 
+// Arrays and element range of one tile.
+template <typename TQ, typename TV, typename TO, typename TC>
+struct TileCtx {
+  const TQ* q;
+  const TV* u;
+  const TV* v;
+  const TV* w;
+  const double* q0;
+  TO* out;
+  const int* pbase;
+  const TC* escale;
+  const TC* fscale;
+  double dt;
+  int e0;  // first element (index into the arrays)
+  int n;   // elements in the tile (1..EPB)
+};
+
+template <int EPB, typename TQ, typename TV, typename TO, typename TC>
+__device__ __forceinline__ TileCtx<TQ, TV, TO, TC> tile_ctx(const TendArgs<TQ, TV, TO, TC>& A,
+                                                            int tile) {
+  TileCtx<TQ, TV, TO, TC> c;
+  if (A.tiles == nullptr) {
+    c.q = A.q;
+    c.u = A.u;
+    c.v = A.v;
+    c.w = A.w;
+    c.q0 = A.q0;
+    c.out = A.out;
+    c.pbase = A.pbase;
+    c.escale = A.escale;
+    c.fscale = A.fscale;
+    c.dt = A.dt;
+    c.e0 = A.elem0 + tile * EPB;
+    c.n = min(EPB, A.nelem - tile * EPB);
+  } else {
+    const BatchTile t = A.tiles[tile];
+    const BatchInst& I = A.insts[t.inst];
+    c.q = static_cast<const TQ*>(I.q);
+    c.u = static_cast<const TV*>(I.u);
+    c.v = static_cast<const TV*>(I.v);
+    c.w = static_cast<const TV*>(I.w);
+    c.q0 = I.q0;
+    c.out = static_cast<TO*>(I.out);
+    c.pbase = I.pbase;
+    c.escale = static_cast<const TC*>(I.escale);
+    c.fscale = static_cast<const TC*>(I.fscale);
+    c.dt = I.dt;
+    c.e0 = t.e0;
+    c.n = t.n;
+  }
+  return c;
+}
+
+// Plus-side node of face f (0-based) at face node (a,b) of the neighbour
+// starting at node p >= 0: Fmask(fp, oppface) - 1 (mod_mesh.f90:278-324).
+template <int NQ>
+__device__ __forceinline__ int opp_offset(int f, int a, int b) {
+  constexpr int NQ2 = NQ * NQ;
+  switch (f) {
+    case 0: return a + NQ * (NQ - 1) + NQ2 * b;   // opposite face 3 (j = Nq)
+    case 1: return NQ * a + NQ2 * b;              // opposite face 4 (i = 1)
+    case 2: return a + NQ2 * b;                   // opposite face 1 (j = 1)
+    case 3: return (NQ - 1) + NQ * a + NQ2 * b;   // opposite face 2 (i = Nq)
+    case 4: return a + NQ * b + NQ2 * (NQ - 1);   // opposite face 6 (k = Nq)
+    default: return a + NQ * b;                   // opposite face 5 (k = 1)
+  }
+}
+
+// Phase 4 of one thread: z-derivative, lift, combine and store for the
+// column nodes k = K0 .. K0+KH-1 (K0 compile-time, so D's rows are
+// immediate constant-bank operands).
+template <int NQ, int K0, int KH, int ORDER, bool STAGE, bool LIFT_REGS, bool EXACT,
+          typename TQ, typename TV, typename TO, typename TC>
+__device__ __forceinline__ void column_epilogue(
+    const TendArgs<TQ, TV, TO, TC>& A, const DMat<NQ, TC>& D,
+    const TileCtx<TQ, TV, TO, TC>& C, int e, long base, int t, int a, int b, const TC* zcol,
+    const TC* sX, const TC* sY, const TC* fQ, TC f5, TC f6, const TC* qc, const double* qs,
+    const double* q0v, const TC* lreg) {
+  constexpr int NQ2 = NQ * NQ;
+  constexpr int NP = NQ2 * NQ;
+  constexpr int RS = Geo<NQ>::RS;
+  constexpr int PS = Geo<NQ>::PS;
+  using AR = Ar<TC, EXACT>;
+  const TC* es = C.escale + 3 * static_cast<long>(e);
+  const TC e1 = es[0], e2 = es[1], e3 = es[2];
+#pragma unroll
+  for (int kk = 0; kk < KH; ++kk) {
+    const int k = K0 + kk;
+    const TC dz = contract<NQ, ORDER, AR, TC>([&](int l) { return zcol[l]; },
+                                              [&](int l) { return D.d[k * NQ + l]; });
+    TC L[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if constexpr (LIFT_REGS) L[f] = lreg[6 * kk + f];
+      else L[f] = ldro(A.lift + t + NQ2 * k + NP * f);
+    }
+    TC lf = AR::mul(L[0], fQ[0 * NQ2 + a + NQ * k]);
+    lf = AR::mad(L[1], fQ[1 * NQ2 + b + NQ * k], lf);
+    lf = AR::mad(L[2], fQ[2 * NQ2 + a + NQ * k], lf);
+    lf = AR::mad(L[3], fQ[3 * NQ2 + b + NQ * k], lf);
+    lf = AR::mad(L[4], f5, lf);
+    lf = AR::mad(L[5], f6, lf);
+    TC acc = AR::mul(e1, sX[a + RS * b + PS * k]);
+    acc = AR::mad(e2, sY[a + RS * b + PS * k], acc);
+    acc = AR::mad(e3, dz, acc);
+    acc = AR::add(acc, lf);
+    const TC dqdt = -acc;
+    const long n = base + t + NQ2 * k;
+    if constexpr (!STAGE) {
+      C.out[n] = static_cast<TO>(dqdt);
+    } else {
+      using AD = Ar<double, EXACT>;
+      double qd;
+      if constexpr (sizeof(TQ) == sizeof(TC)) qd = static_cast<double>(qc[kk]);
+      else qd = qs[kk];
+      double r = AD::mul(A.rk_b, AD::mad(C.dt, static_cast<double>(dqdt), qd));
+      if (A.rk_a != 0.0) r = AD::mad(A.rk_a, q0v[kk], r);
+      C.out[n] = static_cast<TO>(r);
+    }
+  }
+}
+
 template <int NQ, typename TQ, typename TV, typename TO, typename TC, bool EXACT,
           int ORDER, bool STAGE>
-__global__ void __launch_bounds__(Geo<NQ>::THREADS)
+__global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
     tend_pipe_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
                      const __grid_constant__ DMat<NQ, TC> D) {
-  using G = Geo<NQ>;
+  using G = PipeGeo<NQ>;
   using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
   using AR = Ar<TC, EXACT>;
+  using Ctx = TileCtx<TQ, TV, TO, TC>;
   constexpr int NQ2 = G::NQ2;
   constexpr int NP = G::NP;
   constexpr int RS = G::RS;
   constexpr int PS = G::PS;
   constexpr int EPB = G::EPB;
+  constexpr int H = G::H;
+  constexpr int KH = G::KH;
   constexpr int NS = P::NSTAGE;
+  constexpr int NFACE = 4 / H;   // x/y faces evaluated per thread
+  constexpr int NZF = 2 / H;     // z faces evaluated per thread
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* slots = smem_raw;
   TC* work = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::WORK);
 
-  const int s = threadIdx.x / NQ2;
-  const int t = threadIdx.x - s * NQ2;
+  const int s = threadIdx.x / G::TPE;            // element slot
+  const int r = threadIdx.x - s * G::TPE;
+  const int h = (H == 2) ? r / NQ2 : 0;          // warp-uniform half
+  const int t = r - h * NQ2;                     // column index a + NQ*b
   const int a = t % NQ;
   const int b = t / NQ;
-  const int ntiles = (A.nelem + EPB - 1) / EPB;
+  const int k0 = h * KH;
+  const int ntiles = A.tiles ? A.ntiles : (A.nelem + EPB - 1) / EPB;
 
-  TC* sX = work + s * SmemLayout<NQ, TC>::PER_ELEM;
+  TC* sX = work + s * G::WORK_ELEM;
   TC* sY = sX + G::SBUF;
-  TC* fQ = sY + G::SBUF;
-  TC* fU = fQ + 4 * NQ2;
+  TC* fQ = sY + G::SBUF;       // [4][NQ2]
+  TC* fU = fQ + 4 * NQ2;       // [4][NQ2]
+  TC* fZ = fU + 4 * NQ2;       // [2][NQ2] z-face fluxes
+  TC* sZ = fZ + 2 * NQ2;       // [NQ][NQ2] z-column exchange (H = 2)
 
-  // Byte range of the tile's elements in an array of element size `sz`,
+  // Byte range of elements [e0, e0+n) in an array of element size `sz`,
   // widened to 16-byte boundaries.
-  auto range = [&](int tile, size_t sz, size_t* lo16, uint32_t* bytes, uint32_t* shift) {
-    const int e0 = A.elem0 + tile * EPB;
-    const int n = min(EPB, A.nelem - tile * EPB);
+  auto range = [&](int e0, int n, size_t sz, size_t* lo16, uint32_t* bytes,
+                   uint32_t* shift) {
     const size_t lo = static_cast<size_t>(e0) * NP * sz;
     const size_t hi = static_cast<size_t>(e0 + n) * NP * sz;
     *lo16 = lo & ~size_t(15);
@@ -143,19 +318,19 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
 
   // Producer: one thread fills ring slot `slot` with tile `tile`.
   auto issue = [&](int tile, int slot) {
+    const Ctx c = tile_ctx<EPB>(A, tile);
     unsigned char* base = slots + slot * P::SLOT;
-    const void* src[5] = {A.q, A.u, A.v, A.w, A.q0};
-    const size_t sz[5] = {sizeof(TQ), sizeof(TV), sizeof(TV), sizeof(TV), sizeof(double)};
-    const size_t off[5] = {0, P::QB, P::QB + P::VB, P::QB + 2 * P::VB, P::QB + 3 * P::VB};
-    const int narr = (STAGE && A.rk_a != 0.0) ? 5 : 4;
-    size_t lo[5];
-    uint32_t by[5], sh[5], total = 0;
-    for (int k = 0; k < narr; ++k) {
-      range(tile, sz[k], &lo[k], &by[k], &sh[k]);
+    const void* src[4] = {c.q, c.u, c.v, c.w};
+    const size_t sz[4] = {sizeof(TQ), sizeof(TV), sizeof(TV), sizeof(TV)};
+    const size_t off[4] = {0, P::QB, P::QB + P::VB, P::QB + 2 * P::VB};
+    size_t lo[4];
+    uint32_t by[4], sh[4], total = 0;
+    for (int k = 0; k < 4; ++k) {
+      range(c.e0, c.n, sz[k], &lo[k], &by[k], &sh[k]);
       total += by[k];
     }
     mbar_arrive_expect_tx(&bars[slot], total);
-    for (int k = 0; k < narr; ++k)
+    for (int k = 0; k < 4; ++k)
       bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
                &bars[slot]);
   };
@@ -171,14 +346,15 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
       if (tile < ntiles) issue(tile, k);
     }
 
-  // Lift coefficients of this column, kept for the whole loop (p <= 7).
-  constexpr int LR = P::LIFT_REGS ? 6 * NQ : 1;
+  // Lift coefficients of this thread's column nodes, kept for the loop.
+  constexpr int LR = P::LIFT_REGS ? 6 * KH : 1;
   TC lreg[LR];
   if constexpr (P::LIFT_REGS) {
 #pragma unroll
-    for (int k = 0; k < NQ; ++k)
+    for (int kk = 0; kk < KH; ++kk)
 #pragma unroll
-      for (int f = 0; f < 6; ++f) lreg[6 * k + f] = ldro(A.lift + t + NQ2 * k + NP * f);
+      for (int f = 0; f < 6; ++f)
+        lreg[6 * kk + f] = ldro(A.lift + t + NQ2 * (k0 + kk) + NP * f);
   }
 
   for (int it = 0;; ++it) {
@@ -186,40 +362,39 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
     if (tile >= ntiles) break;
     const int slot = it % NS;
     const uint32_t parity = (it / NS) & 1;
-    const int el = tile * EPB + s;
-    const bool active = el < A.nelem;
-    const int e = A.elem0 + (active ? el : 0);
+    const Ctx C = tile_ctx<EPB>(A, tile);
+    const bool active = s < C.n;
+    const int e = C.e0 + (active ? s : 0);
     const long base = static_cast<long>(e) * NP;
 
-    // ---- Plus-side face gathers, issued before the ring wait ---------------
-    TC qP[4], unP[4], q5 = TC(0), w5 = TC(0), q6 = TC(0), w6 = TC(0);
+    // ---- Loads issued before the ring wait: plus-side faces, q0 ---------
+    TC qP[NFACE], unP[NFACE], qZ[NZF], wZ[NZF];
+    double q0v[STAGE ? KH : 1];
     if (active) {
-      const int* pb = A.pbase + 6 * static_cast<long>(e);
+      const int* pb = C.pbase + 6 * static_cast<long>(e);
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
+      for (int ff = 0; ff < NFACE; ++ff) {
+        const int f = h * NFACE + ff;
         const int p = pb[f];
-        long idx;
-        if (p >= 0) {
-          const int off = (f == 0)   ? a + NQ * (NQ - 1) + NQ2 * b
-                          : (f == 1) ? NQ * a + NQ2 * b
-                          : (f == 2) ? a + NQ2 * b
-                                     : (NQ - 1) + NQ * a + NQ2 * b;
-          idx = static_cast<long>(p) + off;
-        } else {
-          idx = static_cast<long>(-1 - p) + t;
-        }
-        qP[f] = static_cast<TC>(ldro(A.q + idx));
-        unP[f] = static_cast<TC>((f == 1 || f == 3) ? ldro(A.u + idx) : ldro(A.v + idx));
+        const long idx = (p >= 0) ? static_cast<long>(p) + opp_offset<NQ>(f, a, b)
+                                  : static_cast<long>(-1 - p) + t;
+        qP[ff] = static_cast<TC>(ldro(C.q + idx));
+        unP[ff] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx) : ldro(C.v + idx));
       }
-      const int p5 = pb[4];
-      const long i5 = (p5 >= 0) ? static_cast<long>(p5) + t + NQ2 * (NQ - 1)
-                                : static_cast<long>(-1 - p5) + t;
-      q5 = static_cast<TC>(ldro(A.q + i5));
-      w5 = static_cast<TC>(ldro(A.w + i5));
-      const int p6 = pb[5];
-      const long i6 = (p6 >= 0) ? static_cast<long>(p6) + t : static_cast<long>(-1 - p6) + t;
-      q6 = static_cast<TC>(ldro(A.q + i6));
-      w6 = static_cast<TC>(ldro(A.w + i6));
+#pragma unroll
+      for (int zz = 0; zz < NZF; ++zz) {
+        const int f = 4 + h * NZF + zz;
+        const int p = pb[f];
+        const long idx = (p >= 0) ? static_cast<long>(p) + opp_offset<NQ>(f, a, b)
+                                  : static_cast<long>(-1 - p) + t;
+        qZ[zz] = static_cast<TC>(ldro(C.q + idx));
+        wZ[zz] = static_cast<TC>(ldro(C.w + idx));
+      }
+      if constexpr (STAGE) {
+#pragma unroll
+        for (int kk = 0; kk < KH; ++kk)
+          q0v[kk] = (A.rk_a != 0.0) ? C.q0[base + t + NQ2 * (k0 + kk)] : 0.0;
+      }
     }
 
     // ---- Wait for the tile's slot (bounded, block-uniform) -----------------
@@ -237,40 +412,37 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
       return;
     }
 
-    // ---- Phase 1: read the column out of the slot -------------------------
+    // ---- Phase 1: read this thread's column nodes out of the slot ---------
     unsigned char* sb = slots + slot * P::SLOT;
     size_t lo;
-    uint32_t by, shq, shv, sh0 = 0;
-    range(tile, sizeof(TQ), &lo, &by, &shq);
-    range(tile, sizeof(TV), &lo, &by, &shv);
-    if (STAGE) range(tile, sizeof(double), &lo, &by, &sh0);
+    uint32_t by, shq, shv;
+    range(C.e0, C.n, sizeof(TQ), &lo, &by, &shq);
+    range(C.e0, C.n, sizeof(TV), &lo, &by, &shv);
     const TQ* sq = reinterpret_cast<const TQ*>(sb + shq) + s * NP;
     const TV* su = reinterpret_cast<const TV*>(sb + P::QB + shv) + s * NP;
     const TV* sv = reinterpret_cast<const TV*>(sb + P::QB + P::VB + shv) + s * NP;
     const TV* sw = reinterpret_cast<const TV*>(sb + P::QB + 2 * P::VB + shv) + s * NP;
-    const double* sq0 =
-        reinterpret_cast<const double*>(sb + P::QB + 3 * P::VB + sh0) + s * NP;
 
-    TC qc[NQ], fz[NQ];
-    double qs[STAGE && sizeof(TQ) != sizeof(TC) ? NQ : 1];
-    double q0v[STAGE ? NQ : 1];
-    TC wlo = TC(0), whi = TC(0);
+    TC qc[KH], fz[KH];
+    double qs[STAGE && sizeof(TQ) != sizeof(TC) ? KH : 1];
+    TC wM[NZF];
     if (active) {
 #pragma unroll
-      for (int k = 0; k < NQ; ++k) {
+      for (int kk = 0; kk < KH; ++kk) {
+        const int k = k0 + kk;
         const int n = t + NQ2 * k;
         const TC qv = static_cast<TC>(sq[n]);
         const TC uv = static_cast<TC>(su[n]);
         const TC vv = static_cast<TC>(sv[n]);
         const TC wv = static_cast<TC>(sw[n]);
-        if constexpr (STAGE && sizeof(TQ) != sizeof(TC)) qs[k] = static_cast<double>(sq[n]);
-        if constexpr (STAGE) q0v[k] = (A.rk_a != 0.0) ? sq0[n] : 0.0;
-        qc[k] = qv;
+        if constexpr (STAGE && sizeof(TQ) != sizeof(TC)) qs[kk] = static_cast<double>(sq[n]);
+        qc[kk] = qv;
         sX[a + RS * b + PS * k] = AR::mul(qv, uv);
         sY[a + RS * b + PS * k] = AR::mul(qv, vv);
-        fz[k] = AR::mul(qv, wv);
-        if (k == 0) wlo = wv;
-        if (k == NQ - 1) whi = wv;
+        fz[kk] = AR::mul(qv, wv);
+        if constexpr (H == 2) sZ[t + NQ2 * k] = fz[kk];
+        if (kk == 0 && k == 0) wM[0] = wv;                 // -z face (k = 1)
+        if (kk == KH - 1 && k == NQ - 1) wM[NZF - 1] = wv;  // +z face (k = Nq)
         if (b == 0)      { fQ[0 * NQ2 + a + NQ * k] = qv; fU[0 * NQ2 + a + NQ * k] = vv; }
         if (a == NQ - 1) { fQ[1 * NQ2 + b + NQ * k] = qv; fU[1 * NQ2 + b + NQ * k] = uv; }
         if (b == NQ - 1) { fQ[2 * NQ2 + a + NQ * k] = qv; fU[2 * NQ2 + a + NQ * k] = vv; }
@@ -284,73 +456,61 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS)
       if (nt < ntiles) issue(nt, slot);
     }
 
-    TC f5 = TC(0), f6 = TC(0);
     if (active) {
-      const TC* fs = A.fscale + 6 * static_cast<long>(e);
+      // ---- Phase 2: face fluxes -------------------------------------------
+      const TC* fs = C.fscale + 6 * static_cast<long>(e);
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
+      for (int ff = 0; ff < NFACE; ++ff) {
+        const int f = h * NFACE + ff;
         const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
         fQ[f * NQ2 + t] =
-            upwind_flux<AR, TC>(fQ[f * NQ2 + t], fU[f * NQ2 + t], qP[f], unP[f], sg, fs[f]);
+            upwind_flux<AR, TC>(fQ[f * NQ2 + t], fU[f * NQ2 + t], qP[ff], unP[ff], sg, fs[f]);
       }
-      f5 = upwind_flux<AR, TC>(qc[0], wlo, q5, w5, TC(-1), fs[4]);
-      f6 = upwind_flux<AR, TC>(qc[NQ - 1], whi, q6, w6, TC(1), fs[5]);
+#pragma unroll
+      for (int zz = 0; zz < NZF; ++zz) {
+        const int f = 4 + h * NZF + zz;   // 4: -z (k = 1), 5: +z (k = Nq)
+        const TC qm = (f == 4) ? qc[0] : qc[KH - 1];
+        fZ[(f - 4) * NQ2 + t] =
+            upwind_flux<AR, TC>(qm, wM[zz], qZ[zz], wZ[zz], f == 4 ? TC(-1) : TC(1), fs[f]);
+      }
+      // ---- Phase 3: line contractions (x-line for h = 0, y-line for h = 1)
       TC line[NQ];
+      if (H == 1 || h == 0) {
 #pragma unroll
-      for (int l = 0; l < NQ; ++l) line[l] = sX[l + RS * a + PS * b];
+        for (int l = 0; l < NQ; ++l) line[l] = sX[l + RS * a + PS * b];
 #pragma unroll
-      for (int i = 0; i < NQ; ++i)
-        sX[i + RS * a + PS * b] = contract<NQ, ORDER, AR, TC>(
-            [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+        for (int i = 0; i < NQ; ++i)
+          sX[i + RS * a + PS * b] = contract<NQ, ORDER, AR, TC>(
+              [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+      }
+      if (H == 1 || h == 1) {
 #pragma unroll
-      for (int l = 0; l < NQ; ++l) line[l] = sY[a + RS * l + PS * b];
+        for (int l = 0; l < NQ; ++l) line[l] = sY[a + RS * l + PS * b];
 #pragma unroll
-      for (int j = 0; j < NQ; ++j)
-        sY[a + RS * j + PS * b] = contract<NQ, ORDER, AR, TC>(
-            [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+        for (int j = 0; j < NQ; ++j)
+          sY[a + RS * j + PS * b] = contract<NQ, ORDER, AR, TC>(
+              [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+      }
     }
     __syncthreads();
 
     if (active) {
-      TC dz[NQ];
+      // ---- Phase 4: z-derivative, lift, combine, store ---------------------
+      TC zcol[NQ];
+      if constexpr (H == 2) {
 #pragma unroll
-      for (int k = 0; k < NQ; ++k)
-        dz[k] = contract<NQ, ORDER, AR, TC>([&](int l) { return fz[l]; },
-                                            [&](int l) { return D.d[k * NQ + l]; });
-      const TC* es = A.escale + 3 * static_cast<long>(e);
-      const TC e1 = es[0], e2 = es[1], e3 = es[2];
+        for (int l = 0; l < NQ; ++l) zcol[l] = sZ[t + NQ2 * l];
+      } else {
 #pragma unroll
-      for (int k = 0; k < NQ; ++k) {
-        TC L[6];
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-          if constexpr (P::LIFT_REGS) L[f] = lreg[6 * k + f];
-          else L[f] = ldro(A.lift + t + NQ2 * k + NP * f);
-        }
-        TC lf = AR::mul(L[0], fQ[0 * NQ2 + a + NQ * k]);
-        lf = AR::mad(L[1], fQ[1 * NQ2 + b + NQ * k], lf);
-        lf = AR::mad(L[2], fQ[2 * NQ2 + a + NQ * k], lf);
-        lf = AR::mad(L[3], fQ[3 * NQ2 + b + NQ * k], lf);
-        lf = AR::mad(L[4], f5, lf);
-        lf = AR::mad(L[5], f6, lf);
-        TC acc = AR::mul(e1, sX[a + RS * b + PS * k]);
-        acc = AR::mad(e2, sY[a + RS * b + PS * k], acc);
-        acc = AR::mad(e3, dz[k], acc);
-        acc = AR::add(acc, lf);
-        const TC dqdt = -acc;
-        const long n = base + t + NQ2 * k;
-        if constexpr (!STAGE) {
-          A.out[n] = static_cast<TO>(dqdt);
-        } else {
-          using AD = Ar<double, EXACT>;
-          double qd;
-          if constexpr (sizeof(TQ) == sizeof(TC)) qd = static_cast<double>(qc[k]);
-          else qd = qs[k];
-          double r = AD::mul(A.rk_b, AD::mad(A.dt, static_cast<double>(dqdt), qd));
-          if (A.rk_a != 0.0) r = AD::mad(A.rk_a, q0v[k], r);
-          A.out[n] = static_cast<TO>(r);
-        }
+        for (int l = 0; l < NQ; ++l) zcol[l] = fz[l];
       }
+      const TC f5 = fZ[t], f6 = fZ[NQ2 + t];
+      if (H == 1 || h == 0)
+        column_epilogue<NQ, 0, KH, ORDER, STAGE, P::LIFT_REGS, EXACT>(
+            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, qc, qs, q0v, lreg);
+      else
+        column_epilogue<NQ, (H == 2 ? KH : 0), KH, ORDER, STAGE, P::LIFT_REGS, EXACT>(
+            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, qc, qs, q0v, lreg);
     }
   }
 }

@@ -78,6 +78,22 @@ SIGNATURES = {
     "sdg_launch_count": (_LL, [_P]),
     "sdg_set_kernel_variant": (_I, [_P, _I]),
     "sdg_minmax_dev_noalloc": (_I, [_P, _LL, _P, _P]),
+    "sdg_batch_create": (_I, [ctypes.POINTER(_P), _I]),
+    "sdg_batch_add": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _D,
+                           ctypes.POINTER(_I)]),
+    "sdg_batch_commit": (_I, [_P, _I]),
+    "sdg_batch_run": (_I, [_P, _I]),
+    "sdg_batch_get": (_I, [_P, _I, _P]),
+    "sdg_batch_info": (_I, [_P, _P, _I]),
+    "sdg_batch_destroy": (_I, [_P]),
+    "sdg_serve_create": (_I, [ctypes.POINTER(_P), _D]),
+    "sdg_serve_submit": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _D, _I, _I,
+                              ctypes.POINTER(_I)]),
+    "sdg_serve_poll": (_I, [_P, _I, ctypes.POINTER(_I), _P]),
+    "sdg_serve_result": (_I, [_P, _I, _P]),
+    "sdg_serve_wait": (_I, [_P, _D]),
+    "sdg_serve_stats": (_I, [_P, _P]),
+    "sdg_serve_destroy": (_I, [_P]),
 }
 
 
@@ -395,3 +411,116 @@ class Problem:
 
     def close(self):
         self.handle.close()
+
+
+# ---------------------------------------------------------------------------
+# Batched ensembles and the serving loop
+# ---------------------------------------------------------------------------
+class Batch:
+    """Many periodic-box instances advanced together (sdg_batch_*)."""
+
+    def __init__(self, flags=0):
+        self._b = ctypes.c_void_p()
+        _check(lib().sdg_batch_create(ctypes.byref(self._b), flags))
+        self.shapes = []
+
+    def add(self, NeX, NeY, NeZ, p, ops, q, u, v, w, dt):
+        """Adds an instance; q,u,v,w are (Np, Ne) or (Np, NeA) arrays."""
+        n = (p + 1) ** 3 * NeX * NeY * NeZ
+        arrs = [_f64(a).reshape(-1, order="F")[:n].copy() for a in (q, u, v, w)]
+        i = ctypes.c_int()
+        _check(lib().sdg_batch_add(self._b, NeX, NeY, NeZ, p, _p(_f64(ops.D1D)),
+                                   _p(_f64(ops.Lift_mat)), *[_p(a) for a in arrs], dt,
+                                   ctypes.byref(i)))
+        self.shapes.append(((p + 1) ** 3, NeX * NeY * NeZ))
+        return i.value
+
+    def commit(self, autotune=True):
+        _check(lib().sdg_batch_commit(self._b, 1 if autotune else 0))
+
+    def run(self, nsteps):
+        _check(lib().sdg_batch_run(self._b, nsteps))
+
+    def get(self, i):
+        np_, ne = self.shapes[i]
+        out = np.zeros((np_, ne), order="F")
+        _check(lib().sdg_batch_get(self._b, i, _p(out)))
+        return out
+
+    def info(self):
+        buf = np.zeros(512)
+        n = lib().sdg_batch_info(self._b, _p(buf), 512)
+        v = buf[:n]
+        groups = []
+        for g in range(int(v[4])):
+            r = v[5 + 7 * g: 12 + 7 * g]
+            groups.append({"p": int(r[0]), "mixed": bool(r[1]), "tiles": int(r[2]),
+                           "variant": int(r[3]), "ms_pipe": r[4], "ms_block": r[5],
+                           "ms_block8": r[6]})
+        return {"instances": int(v[0]), "dof": int(v[1]), "run_s": v[2],
+                "dof_steps": int(v[3]), "groups": groups}
+
+    def close(self):
+        if self._b:
+            _check(lib().sdg_batch_destroy(self._b))
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+SERVE_QUEUED, SERVE_RUNNING, SERVE_DONE, SERVE_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """The serving loop (sdg_serve_*): submit requests, poll, fetch results."""
+
+    def __init__(self, max_bytes=0.0):
+        self._s = ctypes.c_void_p()
+        _check(lib().sdg_serve_create(ctypes.byref(self._s), float(max_bytes)))
+        self.shapes = {}
+
+    def submit(self, NeX, NeY, NeZ, p, ops, q, u, v, w, dt, nsteps, mixed=False):
+        n = (p + 1) ** 3 * NeX * NeY * NeZ
+        arrs = [np.ascontiguousarray(_f64(a).reshape(-1, order="F")[:n]) for a in (q, u, v, w)]
+        i = ctypes.c_int()
+        _check(lib().sdg_serve_submit(self._s, NeX, NeY, NeZ, p, _p(_f64(ops.D1D)),
+                                      _p(_f64(ops.Lift_mat)), *[_p(a) for a in arrs], dt,
+                                      nsteps, FLAG_MIXED if mixed else 0, ctypes.byref(i)))
+        self.shapes[i.value] = ((p + 1) ** 3, NeX * NeY * NeZ)
+        return i.value
+
+    def poll(self, i):
+        st = ctypes.c_int()
+        t = np.zeros(2)
+        _check(lib().sdg_serve_poll(self._s, i, ctypes.byref(st), _p(t)))
+        return st.value, t[0], t[1]
+
+    def result(self, i):
+        np_, ne = self.shapes[i]
+        out = np.zeros((np_, ne), order="F")
+        _check(lib().sdg_serve_result(self._s, i, _p(out)))
+        return out
+
+    def wait(self, timeout_s=0.0):
+        _check(lib().sdg_serve_wait(self._s, float(timeout_s)))
+
+    def stats(self):
+        out = np.zeros(4)
+        _check(lib().sdg_serve_stats(self._s, _p(out)))
+        return {"busy_s": out[0], "dof_steps": out[1], "iterations": int(out[2]),
+                "bytes_in_use": out[3]}
+
+    def close(self):
+        if self._s:
+            _check(lib().sdg_serve_destroy(self._s))
+            self._s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

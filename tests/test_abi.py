@@ -139,6 +139,22 @@ def test_no_cpu_fallback_without_device():
     assert "no CUDA device" in str(e.value)
 
 
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_ensembles_fail_loudly_without_device():
+    with pytest.raises(sdg.SdgError) as e:
+        sdg.Batch(0)
+    assert e.value.code == sdg.SDG_ERR_CUDA
+    with pytest.raises(sdg.SdgError) as e:
+        sdg.Server()
+    assert e.value.code == sdg.SDG_ERR_CUDA
+
+
+def test_ensemble_argument_errors():
+    with pytest.raises(sdg.SdgError) as e:
+        sdg.Batch(sdg.FLAG_MIXED | sdg.FLAG_EXACT)
+    assert e.value.code == sdg.SDG_ERR_ARG
+
+
 def test_evaltype_selector():
     with pytest.raises(sdg.SdgError):
         sdg.dg_optr_kernel_setup("FASTEST")
