@@ -57,7 +57,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fp64_32c_p7", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="fp64_32c_p7",
+                    choices=sorted(WORKLOADS) + ["batch_fp64", "batch_mixed", "served"])
+    ap.add_argument("--requests", type=int, default=200,
+                    help="served workload: number of requests in the stream")
+    ap.add_argument("--seq-sample", type=int, default=12,
+                    help="served workload: requests solved one at a time for comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="budget of the CPU-baseline sample")
@@ -390,10 +395,134 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def ensemble_instances(n, seed, ne_range, p_choices, rng_nstep=None):
+    """Seeded instance list: cubic boxes Ne ~ U{ne_range}, p from p_choices,
+    constant velocity U[-1,1]^3, dt = 0.1 h / (p+1)^2."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        ne = int(rng.integers(ne_range[0], ne_range[1] + 1))
+        p = int(rng.choice(p_choices))
+        nstep = int(rng.integers(rng_nstep[0], rng_nstep[1] + 1)) if rng_nstep else None
+        out.append({"ne": ne, "p": p, "seed": 1000 + k, "nstep": nstep,
+                    "dt": 0.1 / ne / (p + 1) ** 2})
+    return out
+
+
+def run_batch(args):
+    """Batched ensemble: 96 instances, Ne/axis U{6..24}, p in {3,5,7,9},
+    own seeded IC, constant velocity U[-1,1]^3; K RK3 steps of all of them."""
+    import torch
+    import sdg_b200 as sdg
+    mixed = args.workload == "batch_mixed"
+    inst = ensemble_instances(96, 4, (6, 24), [3, 5, 7, 9])
+    b = sdg.Batch(sdg.FLAG_MIXED if mixed else 0)
+    ops = {p: sdg.read_operators(p) for p in (3, 5, 7, 9)}
+    for it in inst:
+        vel = tuple(sdg.random_velocity(it["seed"]))
+        f = sdg.box_fields(it["ne"], it["ne"], it["ne"], it["p"], ops[it["p"]].x1D,
+                           ic_kind=1, seed=it["seed"], vel_kind=0, vel=vel)
+        b.add(it["ne"], it["ne"], it["ne"], it["p"], ops[it["p"]], *f, it["dt"])
+    b.commit(autotune=True)
+    b.run(args.warmup)
+    info0 = b.info()
+    with ClockSampler(0) as clk:
+        b.run(args.steps)
+    info = b.info()
+    t = info["run_s"] - info0["run_s"]
+    dof = info["dof"]
+    value = dof * 3 * args.steps / t
+    groups = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in g.items()}
+              for g in info["groups"]]
+    line = {"metric": "DOF-updates/s per RHS eval", "value": value,
+            "unit": "DOF-updates/s per RHS eval", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "instances": len(inst), "dof_total": dof,
+                       "ne_per_axis": "U{6..24}", "p": [3, 5, 7, 9],
+                       "groups": groups},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    b.close()
+    torch.cuda.synchronize()
+
+
+def run_served(args):
+    """Served request stream: Poisson arrivals at ~80% load; Ne/axis
+    U{8..32}, p U{3..11}, nstep U{50..400}, FP32/FP64 flag.  The stream is
+    shortened to --requests requests (the full 2,000 take ~3 minutes of GPU
+    time at this load); a one-at-a-time FP64 run of the first requests gives
+    the comparison throughput."""
+    import sdg_b200 as sdg
+    reqs = ensemble_instances(args.requests, 5, (8, 32), list(range(3, 12)), (50, 400))
+    rng = np.random.default_rng(6)
+    for r in reqs:
+        r["mixed"] = bool(rng.integers(0, 2))
+    ops = {p: sdg.read_operators(p) for p in range(3, 12)}
+    fields = []
+    for r in reqs:
+        vel = tuple(sdg.random_velocity(r["seed"]))
+        fields.append(sdg.box_fields(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D,
+                                     ic_kind=1, seed=r["seed"], vel_kind=0, vel=vel))
+    work = [r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"] for r in reqs]
+    # Service-rate estimate from the one-at-a-time FP64 solves of a sample.
+    n_seq = min(len(reqs), args.seq_sample)
+    t_seq, w_seq = 0.0, 0
+    for r, f in zip(reqs[:n_seq], fields[:n_seq]):
+        m = sdg.mesh_setup(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D)
+        h = sdg.Handle(ops[r["p"]], m, 0)
+        h.set_state(*f)
+        h.synchronize()
+        t0 = time.perf_counter()
+        h.rk3_steps(r["dt"], r["nstep"])
+        h.synchronize()
+        t_seq += time.perf_counter() - t0
+        w_seq += r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"]
+        h.close()
+        del m
+    seq_rate = w_seq / t_seq
+    mean_work = float(np.mean(work))
+    lam = 0.8 * seq_rate / mean_work           # requests per second at ~80% load
+    gaps = rng.exponential(1.0 / lam, size=len(reqs))
+    srv = sdg.Server()
+    t_start = time.perf_counter()
+    ids = []
+    for r, f, g in zip(reqs, fields, gaps):
+        time.sleep(g)
+        ids.append(srv.submit(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]], *f,
+                              r["dt"], r["nstep"], mixed=r["mixed"]))
+    srv.wait(0)
+    makespan = time.perf_counter() - t_start
+    tts = np.array([srv.poll(i)[2] for i in ids])
+    st = srv.stats()
+    srv.close()
+    total = float(sum(work))
+    line = {"metric": "DOF-updates/s per RHS eval", "value": total / makespan,
+            "unit": "DOF-updates/s per RHS eval", "n_gpus": 1, "steps": len(reqs),
+            "warmup": 0, "ms_per_step": 1e3 * makespan / len(reqs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "served", "requests": len(reqs),
+                       "arrival_rate_per_s": lam, "load": 0.8,
+                       "ne_per_axis": "U{8..32}", "p": "U{3..11}", "nstep": "U{50..400}"},
+            "served": {"p50_tts_s": float(np.percentile(tts, 50)),
+                       "p99_tts_s": float(np.percentile(tts, 99)),
+                       "mean_tts_s": float(tts.mean()), "makespan_s": makespan,
+                       "device_busy_s": st["busy_s"],
+                       "throughput_busy": st["dof_steps"] * 3 / max(st["busy_s"], 1e-9),
+                       "one_at_a_time_fp64": seq_rate, "one_at_a_time_sample": n_seq}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("batch_fp64", "batch_mixed"):
+        run_batch(args)
+    elif args.workload == "served":
+        run_served(args)
     else:
         run_ours(args)
 

@@ -87,7 +87,8 @@ int sdg_fmask(int p, int* Fmask);
 /* mesh_setup (mod_mesh.f90:74-193) for the periodic box
  * [0,domx]x[0,domy]x[0,domz]: VMapM, VMapP (NfpTot,Ne), halo_src_map
  * (NhaloNode), normal_fn (NfpTot,Ne,3), Escale (Np,Ne,3), Fscale (NfpTot,Ne)
- * and pos_en (Np,Ne,3), bit-identical to the reference's tables. */
+ * and pos_en (Np,Ne,3), bit-identical to the reference's tables.  Any
+ * output pointer may be NULL to skip that table. */
 int sdg_mesh_setup(int NeX, int NeY, int NeZ, int p, double domx, double domy,
                    double domz, const double* x1D, int* VMapM, int* VMapP,
                    int* halo_src_map, double* normal_fn, double* Escale,

@@ -221,13 +221,13 @@ int sdg_mesh_setup(int NeX, int NeY, int NeZ, int p, double domx, double domy,
           const int opp = kOppFace[f];
           for (int fp = 0; fp < Nfp; ++fp) {
             const long slot = f * Nfp + fp + NfpTot * e0;
-            VMapM[slot] = face_node(Nq, f, fp) + 1 + (ke - 1) * Np;
+            if (VMapM) VMapM[slot] = face_node(Nq, f, fp) + 1 + (ke - 1) * Np;
             const int src = face_node(Nq, opp, fp) + 1 + (keP - 1) * Np;
             if (wraps) {
               ++ibuf;
-              VMapP[slot] = Np * Ne + ibuf;
+              if (VMapP) VMapP[slot] = Np * Ne + ibuf;
               if (halo_src_map) halo_src_map[ibuf - 1] = src;
-            } else {
+            } else if (VMapP) {
               VMapP[slot] = src;
             }
             if (normal_fn)

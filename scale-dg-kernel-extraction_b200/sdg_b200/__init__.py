@@ -199,6 +199,20 @@ def mesh_setup(NeX, NeY, NeZ, p, x1D, dom=(1.0, 1.0, 1.0)):
                 s["NhaloNode"], VMapM, VMapP, hmap, nfn, Esc, Fsc, pos)
 
 
+def box_fields(NeX, NeY, NeZ, p, x1D, ic_kind=1, seed=0, vel_kind=0, vel=(1.0, 1.0, 1.0)):
+    """Initial q, u, v, w (Np, Ne) of the periodic unit box without building
+    the mesh tables (only the node positions)."""
+    s = mesh_sizes(NeX, NeY, NeZ, p)
+    Np, Ne = s["Np"], s["Ne"]
+    pos = np.zeros((Np, Ne, 3), order="F")
+    _check(lib().sdg_mesh_setup(NeX, NeY, NeZ, p, 1.0, 1.0, 1.0, _p(_f64(x1D)), None, None,
+                                None, None, None, None, _p(pos)))
+    q, u, v, w = (np.zeros((Np, Ne), order="F") for _ in range(4))
+    _check(lib().sdg_init_fields(ic_kind, seed, vel_kind, vel[0], vel[1], vel[2], _p(pos),
+                                 Np, Ne, _p(q), _p(u), _p(v), _p(w)))
+    return q, u, v, w
+
+
 def update_halo(f, mesh):
     """update_halo (mod_mesh.f90:209-221) on a host array, in place."""
     if not (isinstance(f, np.ndarray) and f.dtype == np.float64 and
