@@ -18,6 +18,29 @@ namespace {
 
 constexpr int NQ = SDG_NQ;
 
+// Launches a persistent pipelined kernel: attribute and occupancy set-up on
+// the first call of each instantiation (a call with no tiles only primes
+// it, e.g. before a stream capture), then one block per resident slot.
+template <bool BATCH, typename K, typename Args, typename Dm>
+int launch_pipe(K kern, size_t smem, int ntiles, const LaunchSpec& s, const Args& a,
+                const Dm& d) {
+  static int blocks_per_sm = 0;  // per instantiation; the plan is fixed
+  if (blocks_per_sm == 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return static_cast<int>(e);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, PipeGeo<NQ>::THREADS, smem);
+    if (e != cudaSuccess) return static_cast<int>(e);
+    blocks_per_sm = nb > 0 ? nb : 1;
+  }
+  if (ntiles <= 0) return 0;
+  const int grid = std::min(ntiles, blocks_per_sm * (s.num_sms > 0 ? s.num_sms : 148));
+  kern<<<grid, PipeGeo<NQ>::THREADS, smem, s.stream>>>(a, d);
+  return static_cast<int>(cudaGetLastError());
+}
+
 template <typename TQ, typename TV, typename TO, typename TC, bool EXACT,
           int ORDER, bool STAGE>
 int run(const LaunchSpec& s) {
@@ -56,27 +79,13 @@ int run(const LaunchSpec& s) {
   const bool pipe =
       batch || ((s.variant == kVariantPipe || s.variant == kVariantAuto) && can_pipe);
   if (pipe) {
-    // Attribute and occupancy set-up runs on the first call (a call with
-    // nelem == 0 only primes it, e.g. before a stream capture).
-    auto kern = tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
-    static int blocks_per_sm = 0;  // per instantiation; the plan is fixed
-    if (blocks_per_sm == 0) {
-      cudaError_t e = cudaFuncSetAttribute(
-          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(P::BYTES));
-      if (e != cudaSuccess) return static_cast<int>(e);
-      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-      int nb = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, PipeGeo<NQ>::THREADS,
-                                                        P::BYTES);
-      if (e != cudaSuccess) return static_cast<int>(e);
-      blocks_per_sm = nb > 0 ? nb : 1;
-    }
     const int ntiles =
         batch ? s.batch_ntiles : (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
-    if (ntiles <= 0) return 0;
-    const int grid = std::min(ntiles, blocks_per_sm * (s.num_sms > 0 ? s.num_sms : 148));
-    kern<<<grid, PipeGeo<NQ>::THREADS, P::BYTES, s.stream>>>(a, d);
-    return static_cast<int>(cudaGetLastError());
+    if (batch)
+      return launch_pipe<true>(tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, true>,
+                               P::BYTES, ntiles, s, a, d);
+    return launch_pipe<false>(tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false>,
+                              P::BYTES, ntiles, s, a, d);
   }
 
   const size_t smem = SmemLayout<NQ, TC>::BYTES;

@@ -2,13 +2,15 @@
 // kernel (same arithmetic as tend_kernel in sdg_tend.cuh, same results).
 //
 // Each block loops over tiles of EPB consecutive elements.  The element data
-// a tile needs (q, u, v, w) are contiguous in HBM, so one elected thread moves
-// them into a shared-memory ring of NSTAGE tiles with cp.async.bulk (the TMA
-// bulk-copy engine), completing on an mbarrier per ring slot; the copy of
-// tile i+NSTAGE is issued as soon as tile i has been read out of its slot.
-// Compute threads never stall on their own element loads: the bytes in
-// flight per SM are set by the ring, not by occupancy.  The plus-side face
-// values (in neighbouring elements) and the RK base state q0 are loaded with
+// a tile needs (q, u, v, w and, for RK stages 2-3, q0) are contiguous in
+// HBM, so one elected thread moves them into a shared-memory ring of NSTAGE
+// tiles with cp.async.bulk (the TMA bulk-copy engine), completing on an
+// mbarrier per ring slot.  A slot stays resident for its whole tile (the
+// epilogue re-reads q and q0 from it instead of holding them in registers)
+// and is refilled, with the tile NSTAGE iterations on, as the block starts
+// the next tile.  Compute threads never stall on their own element loads:
+// the bytes in flight per SM are set by the ring, not by occupancy.  The
+// plus-side face values (in neighbouring elements) are gathered with
 // ordinary loads issued before the ring wait, so their latency overlaps it.
 //
 // Thread mapping.  Column (a,b) of an element (its z-line) is owned by H
@@ -102,6 +104,48 @@ __device__ __forceinline__ void fence_barrier_init() {
 #endif
 constexpr bool kSplitColumns = SDG_SPLIT_COLUMNS != 0;
 
+// Placement of node (i,j,k) in the x-line and y-line buffers.  Generic
+// orders use the padded layout of tend_kernel.  For Nq = 8 an XOR swizzle
+// over the 16 eight-byte bank pairs makes every access pattern of the
+// kernel conflict-free: column (i fastest, two j per half-warp), x-line
+// (fixed i, j and two k per half-warp) and y-line (fixed j, i and two k):
+//   x(i,j,k) = 16*((j + 8k) >> 1) + ((i ^ j) & 7) + 8*((j + k) & 1)
+//   y(i,j,k) = 16*((i + 8k) >> 1) + ((i ^ j) & 7) + 8*((i + k) & 1)
+// (bijections onto 0..511).  The padded layout costs two wavefronts more
+// per column access.
+template <int NQ>
+struct LineIdx {
+  static constexpr int SIZE = Geo<NQ>::SBUF;
+  static __device__ __forceinline__ int x(int i, int j, int k) {
+    return i + Geo<NQ>::RS * j + Geo<NQ>::PS * k;
+  }
+  static __device__ __forceinline__ int y(int i, int j, int k) {
+    return i + Geo<NQ>::RS * j + Geo<NQ>::PS * k;
+  }
+};
+template <>
+struct LineIdx<8> {
+  static constexpr int SIZE = 512;
+  static __device__ __forceinline__ int x(int i, int j, int k) {
+    return 16 * ((j + 8 * k) >> 1) + ((i ^ j) & 7) + 8 * ((j + k) & 1);
+  }
+  static __device__ __forceinline__ int y(int i, int j, int k) {
+    return 16 * ((i + 8 * k) >> 1) + ((i ^ j) & 7) + 8 * ((i + k) & 1);
+  }
+};
+
+// A (q_minus, un_minus) pair of a face node, stored in one 8- or 16-byte word.
+template <typename T>
+struct Pair2;
+template <>
+struct Pair2<double> {
+  using type = double2;
+};
+template <>
+struct Pair2<float> {
+  using type = float2;
+};
+
 template <int NQ>
 struct PipeGeo {
   static constexpr int NQ2 = NQ * NQ;
@@ -112,12 +156,11 @@ struct PipeGeo {
   static constexpr int TARGET = (H == 2) ? 256 : 128;
   static constexpr int EPB = TPE >= TARGET ? 1 : TARGET / TPE;
   static constexpr int THREADS = EPB * TPE;
-  static constexpr int RS = Geo<NQ>::RS;
-  static constexpr int PS = Geo<NQ>::PS;
-  static constexpr int SBUF = Geo<NQ>::SBUF;
-  // Per-element work area: x- and y-line buffers, the four x/y faces'
-  // (q_minus, un_minus) pairs (the flux overwrites q_minus), the two z-face
-  // fluxes and, when H = 2, the z-column exchange buffer.
+  static constexpr int SBUF = LineIdx<NQ>::SIZE;
+  // Per-element work area (in compute-type words): x- and y-line buffers,
+  // the four x/y faces' (q_minus, un_minus) pairs (each face flux
+  // overwrites its q_minus), the two z-face fluxes and, when H = 2, the
+  // z-column exchange buffer.
   static constexpr int WORK_ELEM = 2 * SBUF + 8 * NQ2 + 2 * NQ2 + (H == 2 ? NP : 0);
 };
 
@@ -134,7 +177,8 @@ struct PipePlan {
   // each for 4- and 8-byte elements).
   static constexpr size_t QB = r16(sizeof(TQ) * EPB * NP + 32);
   static constexpr size_t VB = r16(sizeof(TV) * EPB * NP + 32);
-  static constexpr size_t SLOT = QB + 3 * VB;
+  static constexpr size_t Q0B = STAGE ? r16(sizeof(double) * EPB * NP + 32) : 0;
+  static constexpr size_t SLOT = QB + 3 * VB + Q0B;
   static constexpr size_t WORK = r16(sizeof(TC) * G::WORK_ELEM * EPB);
   static constexpr size_t BARS = 16 * NSTAGE;
   static constexpr size_t BYTES = NSTAGE * SLOT + WORK + BARS;
@@ -159,11 +203,13 @@ struct TileCtx {
   int n;   // elements in the tile (1..EPB)
 };
 
-template <int EPB, typename TQ, typename TV, typename TO, typename TC>
+// BATCH is a compile-time property of the kernel, so a single-instance
+// launch keeps its pointers in the parameter bank instead of registers.
+template <int EPB, bool BATCH, typename TQ, typename TV, typename TO, typename TC>
 __device__ __forceinline__ TileCtx<TQ, TV, TO, TC> tile_ctx(const TendArgs<TQ, TV, TO, TC>& A,
                                                             int tile) {
   TileCtx<TQ, TV, TO, TC> c;
-  if (A.tiles == nullptr) {
+  if constexpr (!BATCH) {
     c.q = A.q;
     c.u = A.u;
     c.v = A.v;
@@ -218,12 +264,11 @@ template <int NQ, int K0, int KH, int ORDER, bool STAGE, bool LIFT_REGS, bool EX
 __device__ __forceinline__ void column_epilogue(
     const TendArgs<TQ, TV, TO, TC>& A, const DMat<NQ, TC>& D,
     const TileCtx<TQ, TV, TO, TC>& C, int e, long base, int t, int a, int b, const TC* zcol,
-    const TC* sX, const TC* sY, const TC* fQ, TC f5, TC f6, const TC* qc, const double* qs,
-    const double* q0v, const TC* lreg) {
+    const TC* sX, const TC* sY, const TC* fQ, TC f5, TC f6, const TQ* sq,
+    const double* sq0, const TC* lreg) {
   constexpr int NQ2 = NQ * NQ;
   constexpr int NP = NQ2 * NQ;
-  constexpr int RS = Geo<NQ>::RS;
-  constexpr int PS = Geo<NQ>::PS;
+  using LI = LineIdx<NQ>;
   using AR = Ar<TC, EXACT>;
   const TC* es = C.escale + 3 * static_cast<long>(e);
   const TC e1 = es[0], e2 = es[1], e3 = es[2];
@@ -238,14 +283,15 @@ __device__ __forceinline__ void column_epilogue(
       if constexpr (LIFT_REGS) L[f] = lreg[6 * kk + f];
       else L[f] = ldro(A.lift + t + NQ2 * k + NP * f);
     }
-    TC lf = AR::mul(L[0], fQ[0 * NQ2 + a + NQ * k]);
-    lf = AR::mad(L[1], fQ[1 * NQ2 + b + NQ * k], lf);
-    lf = AR::mad(L[2], fQ[2 * NQ2 + a + NQ * k], lf);
-    lf = AR::mad(L[3], fQ[3 * NQ2 + b + NQ * k], lf);
+    // x/y face fluxes sit at stride 2 (the .x of each (q, un) pair).
+    TC lf = AR::mul(L[0], fQ[2 * (0 * NQ2 + a + NQ * k)]);
+    lf = AR::mad(L[1], fQ[2 * (1 * NQ2 + b + NQ * k)], lf);
+    lf = AR::mad(L[2], fQ[2 * (2 * NQ2 + a + NQ * k)], lf);
+    lf = AR::mad(L[3], fQ[2 * (3 * NQ2 + b + NQ * k)], lf);
     lf = AR::mad(L[4], f5, lf);
     lf = AR::mad(L[5], f6, lf);
-    TC acc = AR::mul(e1, sX[a + RS * b + PS * k]);
-    acc = AR::mad(e2, sY[a + RS * b + PS * k], acc);
+    TC acc = AR::mul(e1, sX[LI::x(a, b, k)]);
+    acc = AR::mad(e2, sY[LI::y(a, b, k)], acc);
     acc = AR::mad(e3, dz, acc);
     acc = AR::add(acc, lf);
     const TC dqdt = -acc;
@@ -255,17 +301,18 @@ __device__ __forceinline__ void column_epilogue(
     } else {
       using AD = Ar<double, EXACT>;
       double qd;
-      if constexpr (sizeof(TQ) == sizeof(TC)) qd = static_cast<double>(qc[kk]);
-      else qd = qs[kk];
+      // The stage input at its stored precision, from the tile's ring slot.
+      qd = static_cast<double>(sq[t + NQ2 * k]);
       double r = AD::mul(A.rk_b, AD::mad(C.dt, static_cast<double>(dqdt), qd));
-      if (A.rk_a != 0.0) r = AD::mad(A.rk_a, q0v[kk], r);
+      // q0 is read from the tile's ring slot (still resident in phase 4).
+      if (A.rk_a != 0.0) r = AD::mad(A.rk_a, sq0[t + NQ2 * k], r);
       C.out[n] = static_cast<TO>(r);
     }
   }
 }
 
 template <int NQ, typename TQ, typename TV, typename TO, typename TC, bool EXACT,
-          int ORDER, bool STAGE>
+          int ORDER, bool STAGE, bool BATCH>
 __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
     tend_pipe_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
                      const __grid_constant__ DMat<NQ, TC> D) {
@@ -275,8 +322,6 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
   using Ctx = TileCtx<TQ, TV, TO, TC>;
   constexpr int NQ2 = G::NQ2;
   constexpr int NP = G::NP;
-  constexpr int RS = G::RS;
-  constexpr int PS = G::PS;
   constexpr int EPB = G::EPB;
   constexpr int H = G::H;
   constexpr int KH = G::KH;
@@ -296,13 +341,17 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
   const int a = t % NQ;
   const int b = t / NQ;
   const int k0 = h * KH;
-  const int ntiles = A.tiles ? A.ntiles : (A.nelem + EPB - 1) / EPB;
+  const int ntiles = BATCH ? A.ntiles : (A.nelem + EPB - 1) / EPB;
 
+  using V2 = typename Pair2<TC>::type;
+  using LI = LineIdx<NQ>;
   TC* sX = work + s * G::WORK_ELEM;
   TC* sY = sX + G::SBUF;
-  TC* fQ = sY + G::SBUF;       // [4][NQ2]
-  TC* fU = fQ + 4 * NQ2;       // [4][NQ2]
-  TC* fZ = fU + 4 * NQ2;       // [2][NQ2] z-face fluxes
+  // [4][NQ2] (q, un) of the minus side; phase 2 overwrites q with the flux,
+  // so the lift reads the x/y face fluxes at stride 2 from fQ.
+  V2* fM = reinterpret_cast<V2*>(sY + G::SBUF);
+  TC* fQ = sY + G::SBUF;
+  TC* fZ = fQ + 8 * NQ2;       // [2][NQ2] z-face fluxes
   TC* sZ = fZ + 2 * NQ2;       // [NQ][NQ2] z-column exchange (H = 2)
 
   // Byte range of elements [e0, e0+n) in an array of element size `sz`,
@@ -318,19 +367,20 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
 
   // Producer: one thread fills ring slot `slot` with tile `tile`.
   auto issue = [&](int tile, int slot) {
-    const Ctx c = tile_ctx<EPB>(A, tile);
+    const Ctx c = tile_ctx<EPB, BATCH>(A, tile);
     unsigned char* base = slots + slot * P::SLOT;
-    const void* src[4] = {c.q, c.u, c.v, c.w};
-    const size_t sz[4] = {sizeof(TQ), sizeof(TV), sizeof(TV), sizeof(TV)};
-    const size_t off[4] = {0, P::QB, P::QB + P::VB, P::QB + 2 * P::VB};
-    size_t lo[4];
-    uint32_t by[4], sh[4], total = 0;
-    for (int k = 0; k < 4; ++k) {
+    const void* src[5] = {c.q, c.u, c.v, c.w, c.q0};
+    const size_t sz[5] = {sizeof(TQ), sizeof(TV), sizeof(TV), sizeof(TV), sizeof(double)};
+    const size_t off[5] = {0, P::QB, P::QB + P::VB, P::QB + 2 * P::VB, P::QB + 3 * P::VB};
+    const int narr = (STAGE && A.rk_a != 0.0) ? 5 : 4;
+    size_t lo[5];
+    uint32_t by[5], sh[5], total = 0;
+    for (int k = 0; k < narr; ++k) {
       range(c.e0, c.n, sz[k], &lo[k], &by[k], &sh[k]);
       total += by[k];
     }
     mbar_arrive_expect_tx(&bars[slot], total);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < narr; ++k)
       bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
                &bars[slot]);
   };
@@ -362,14 +412,13 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
     if (tile >= ntiles) break;
     const int slot = it % NS;
     const uint32_t parity = (it / NS) & 1;
-    const Ctx C = tile_ctx<EPB>(A, tile);
+    const Ctx C = tile_ctx<EPB, BATCH>(A, tile);
     const bool active = s < C.n;
     const int e = C.e0 + (active ? s : 0);
     const long base = static_cast<long>(e) * NP;
 
-    // ---- Loads issued before the ring wait: plus-side faces, q0 ---------
+    // ---- Plus-side face gathers, issued before the ring wait -------------
     TC qP[NFACE], unP[NFACE], qZ[NZF], wZ[NZF];
-    double q0v[STAGE ? KH : 1];
     if (active) {
       const int* pb = C.pbase + 6 * static_cast<long>(e);
 #pragma unroll
@@ -390,11 +439,6 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
         qZ[zz] = static_cast<TC>(ldro(C.q + idx));
         wZ[zz] = static_cast<TC>(ldro(C.w + idx));
       }
-      if constexpr (STAGE) {
-#pragma unroll
-        for (int kk = 0; kk < KH; ++kk)
-          q0v[kk] = (A.rk_a != 0.0) ? C.q0[base + t + NQ2 * (k0 + kk)] : 0.0;
-      }
     }
 
     // ---- Wait for the tile's slot (bounded, block-uniform) -----------------
@@ -402,14 +446,23 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
     if (!ok) {
       if (threadIdx.x == 0) {
         atomicExch(A.status, kStatusWaitTimeout);
-        // Drain this block's copies still in flight (this slot included)
-        // before leaving.
+        // Drain this block's copies still in flight before leaving: tile it
+        // and, before the first refill, the prologue's other tiles.  A tile
+        // T >= NS is issued in iteration T - NS + 1.
         for (int k = 0; k < NS; ++k) {
-          const int tk = blockIdx.x + (it + k) * gridDim.x;
-          if (tk < ntiles) mbar_wait_bounded(&bars[(it + k) % NS], ((it + k) / NS) & 1);
+          const int T = it + k;
+          const int tk = blockIdx.x + T * gridDim.x;
+          if (tk < ntiles && (T < NS || T - NS + 1 <= it - 1))
+            mbar_wait_bounded(&bars[T % NS], (T / NS) & 1);
         }
       }
       return;
+    }
+    // Every thread finished the previous tile (the barrier above), so its
+    // slot is free: refill it with the tile NS iterations on from it.
+    if (threadIdx.x == 0 && it > 0) {
+      const int nt = blockIdx.x + (it - 1 + NS) * gridDim.x;
+      if (nt < ntiles) issue(nt, (it - 1) % NS);
     }
 
     // ---- Phase 1: read this thread's column nodes out of the slot ---------
@@ -422,9 +475,13 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
     const TV* su = reinterpret_cast<const TV*>(sb + P::QB + shv) + s * NP;
     const TV* sv = reinterpret_cast<const TV*>(sb + P::QB + P::VB + shv) + s * NP;
     const TV* sw = reinterpret_cast<const TV*>(sb + P::QB + 2 * P::VB + shv) + s * NP;
+    uint32_t sh0 = 0;
+    if constexpr (STAGE) range(C.e0, C.n, sizeof(double), &lo, &by, &sh0);
+    const double* sq0 =
+        reinterpret_cast<const double*>(sb + P::QB + 3 * P::VB + sh0) + s * NP;
 
-    TC qc[KH], fz[KH];
-    double qs[STAGE && sizeof(TQ) != sizeof(TC) ? KH : 1];
+    TC fz[KH];
+    TC qlo = TC(0), qhi = TC(0);   // q on the -z and +z faces
     TC wM[NZF];
     if (active) {
 #pragma unroll
@@ -435,26 +492,21 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
         const TC uv = static_cast<TC>(su[n]);
         const TC vv = static_cast<TC>(sv[n]);
         const TC wv = static_cast<TC>(sw[n]);
-        if constexpr (STAGE && sizeof(TQ) != sizeof(TC)) qs[kk] = static_cast<double>(sq[n]);
-        qc[kk] = qv;
-        sX[a + RS * b + PS * k] = AR::mul(qv, uv);
-        sY[a + RS * b + PS * k] = AR::mul(qv, vv);
+        if (kk == 0) qlo = qv;
+        if (kk == KH - 1) qhi = qv;
+        sX[LI::x(a, b, k)] = AR::mul(qv, uv);
+        sY[LI::y(a, b, k)] = AR::mul(qv, vv);
         fz[kk] = AR::mul(qv, wv);
         if constexpr (H == 2) sZ[t + NQ2 * k] = fz[kk];
         if (kk == 0 && k == 0) wM[0] = wv;                 // -z face (k = 1)
         if (kk == KH - 1 && k == NQ - 1) wM[NZF - 1] = wv;  // +z face (k = Nq)
-        if (b == 0)      { fQ[0 * NQ2 + a + NQ * k] = qv; fU[0 * NQ2 + a + NQ * k] = vv; }
-        if (a == NQ - 1) { fQ[1 * NQ2 + b + NQ * k] = qv; fU[1 * NQ2 + b + NQ * k] = uv; }
-        if (b == NQ - 1) { fQ[2 * NQ2 + a + NQ * k] = qv; fU[2 * NQ2 + a + NQ * k] = vv; }
-        if (a == 0)      { fQ[3 * NQ2 + b + NQ * k] = qv; fU[3 * NQ2 + b + NQ * k] = uv; }
+        if (b == 0) fM[0 * NQ2 + a + NQ * k] = V2{qv, vv};
+        if (a == NQ - 1) fM[1 * NQ2 + b + NQ * k] = V2{qv, uv};
+        if (b == NQ - 1) fM[2 * NQ2 + a + NQ * k] = V2{qv, vv};
+        if (a == 0) fM[3 * NQ2 + b + NQ * k] = V2{qv, uv};
       }
     }
     __syncthreads();
-    // The slot has been read out: refill it with the tile NS iterations on.
-    if (threadIdx.x == 0) {
-      const int nt = blockIdx.x + (it + NS) * gridDim.x;
-      if (nt < ntiles) issue(nt, slot);
-    }
 
     if (active) {
       // ---- Phase 2: face fluxes -------------------------------------------
@@ -463,13 +515,13 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
       for (int ff = 0; ff < NFACE; ++ff) {
         const int f = h * NFACE + ff;
         const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
-        fQ[f * NQ2 + t] =
-            upwind_flux<AR, TC>(fQ[f * NQ2 + t], fU[f * NQ2 + t], qP[ff], unP[ff], sg, fs[f]);
+        const V2 m = fM[f * NQ2 + t];
+        fQ[2 * (f * NQ2 + t)] = upwind_flux<AR, TC>(m.x, m.y, qP[ff], unP[ff], sg, fs[f]);
       }
 #pragma unroll
       for (int zz = 0; zz < NZF; ++zz) {
         const int f = 4 + h * NZF + zz;   // 4: -z (k = 1), 5: +z (k = Nq)
-        const TC qm = (f == 4) ? qc[0] : qc[KH - 1];
+        const TC qm = (f == 4) ? qlo : qhi;
         fZ[(f - 4) * NQ2 + t] =
             upwind_flux<AR, TC>(qm, wM[zz], qZ[zz], wZ[zz], f == 4 ? TC(-1) : TC(1), fs[f]);
       }
@@ -477,18 +529,18 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
       TC line[NQ];
       if (H == 1 || h == 0) {
 #pragma unroll
-        for (int l = 0; l < NQ; ++l) line[l] = sX[l + RS * a + PS * b];
+        for (int l = 0; l < NQ; ++l) line[l] = sX[LI::x(l, a, b)];
 #pragma unroll
         for (int i = 0; i < NQ; ++i)
-          sX[i + RS * a + PS * b] = contract<NQ, ORDER, AR, TC>(
+          sX[LI::x(i, a, b)] = contract<NQ, ORDER, AR, TC>(
               [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
       }
       if (H == 1 || h == 1) {
 #pragma unroll
-        for (int l = 0; l < NQ; ++l) line[l] = sY[a + RS * l + PS * b];
+        for (int l = 0; l < NQ; ++l) line[l] = sY[LI::y(a, l, b)];
 #pragma unroll
         for (int j = 0; j < NQ; ++j)
-          sY[a + RS * j + PS * b] = contract<NQ, ORDER, AR, TC>(
+          sY[LI::y(a, j, b)] = contract<NQ, ORDER, AR, TC>(
               [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
       }
     }
@@ -507,10 +559,10 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
       const TC f5 = fZ[t], f6 = fZ[NQ2 + t];
       if (H == 1 || h == 0)
         column_epilogue<NQ, 0, KH, ORDER, STAGE, P::LIFT_REGS, EXACT>(
-            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, qc, qs, q0v, lreg);
+            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, sq, sq0, lreg);
       else
         column_epilogue<NQ, (H == 2 ? KH : 0), KH, ORDER, STAGE, P::LIFT_REGS, EXACT>(
-            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, qc, qs, q0v, lreg);
+            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, sq, sq0, lreg);
     }
   }
 }
