@@ -76,6 +76,59 @@ def dist_env():
     return rank, world, local
 
 
+class Replicas:
+    """One independent replica of the workload per rank (the path has no data
+    exchange between meshes): a process group for the barrier around the
+    timed region and the max over ranks of its duration, nothing on the data
+    path.  `backend` is "nccl" on GPUs; the CPU tests drive it with "gloo"
+    and device "cpu"."""
+
+    def __init__(self, backend="nccl", device="cuda", timeout_s=120):
+        self.rank, self.world, self.local = dist_env()
+        self.device = device
+        self.pg = None
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+            self.pg = dist
+
+    def barrier(self):
+        if self.device == "cuda":
+            import torch
+            torch.cuda.synchronize()
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        """Max of a float over ranks (every rank gets it)."""
+        if not self.pg:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if not self.pg:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def rate(self, units, seconds):
+        """Whole-job throughput: the units all ranks processed over the
+        slowest rank's time."""
+        return self.sum(units) / self.max(seconds)
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+            self.pg = None
+
+
 def measured_peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -250,12 +303,7 @@ def run_ours(args):
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-        pg = dist
+    rep = Replicas("nccl", "cuda")
     import sdg_b200 as sdg
 
     ops, mesh, flags, (q, u, v, w), dt = build_problem(args.workload, sdg)
@@ -265,17 +313,8 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(H.stream())
     dof = mesh.Ne * mesh.Np
 
-    def barrier():
-        torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-
-    def max_over_ranks(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     # ---- warm-up ----
     H.rk3_steps(dt, args.warmup)
@@ -377,7 +416,7 @@ def run_ours(args):
                          "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "traffic": traffic,
-                         "kernel": "tend_kernel (fused flux+volume+lift+RK stage)",
+                         "kernel": "tend_pipe_kernel (fused flux+volume+lift+RK stage)",
                          "stage_ms": stage_ms,
                          "alg_bytes_per_dof": bpd},
             "e2e": {"value": e2e, "unit": "DOF-updates/s per RHS eval",
@@ -390,9 +429,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     H.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    rep.close()
 
 
 def ensemble_instances(n, seed, ne_range, p_choices, rng_nstep=None):
@@ -413,6 +450,9 @@ def run_batch(args):
     """Batched ensemble: 96 instances, Ne/axis U{6..24}, p in {3,5,7,9},
     own seeded IC, constant velocity U[-1,1]^3; K RK3 steps of all of them."""
     import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
     import sdg_b200 as sdg
     mixed = args.workload == "batch_mixed"
     inst = ensemble_instances(96, 4, (6, 24), [3, 5, 7, 9])
@@ -426,26 +466,33 @@ def run_batch(args):
     b.commit(autotune=True)
     b.run(args.warmup)
     info0 = b.info()
-    with ClockSampler(0) as clk:
+    with ClockSampler(local) as clk:
+        rep.barrier()
         b.run(args.steps)
+        rep.barrier()
     info = b.info()
     t = info["run_s"] - info0["run_s"]
     dof = info["dof"]
-    value = dof * 3 * args.steps / t
+    value = rep.rate(dof * 3 * args.steps, t)
+    t = rep.max(t)
     groups = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in g.items()}
               for g in info["groups"]]
+    b.close()
+    torch.cuda.synchronize()
+    rep.close()
+    if rank != 0:
+        return
     line = {"metric": "DOF-updates/s per RHS eval", "value": value,
-            "unit": "DOF-updates/s per RHS eval", "n_gpus": 1, "steps": args.steps,
+            "unit": "DOF-updates/s per RHS eval", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
             "config": {"workload": args.workload, "instances": len(inst), "dof_total": dof,
                        "ne_per_axis": "U{6..24}", "p": [3, 5, 7, 9],
-                       "groups": groups},
+                       "groups": groups,
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
-    b.close()
-    torch.cuda.synchronize()
 
 
 def run_served(args):
@@ -453,7 +500,13 @@ def run_served(args):
     U{8..32}, p U{3..11}, nstep U{50..400}, FP32/FP64 flag.  The stream is
     shortened to --requests requests (the full 2,000 take ~3 minutes of GPU
     time at this load); a one-at-a-time FP64 run of the first requests gives
-    the comparison throughput."""
+    the comparison throughput.  With N ranks each GPU serves its own copy of
+    the stream; the aggregate is all ranks' work over the slowest makespan
+    and the percentiles are the worst rank's."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
     import sdg_b200 as sdg
     reqs = ensemble_instances(args.requests, 5, (8, 32), list(range(3, 12)), (50, 400))
     rng = np.random.default_rng(6)
@@ -486,6 +539,7 @@ def run_served(args):
     lam = 0.8 * seq_rate / mean_work           # requests per second at ~80% load
     gaps = rng.exponential(1.0 / lam, size=len(reqs))
     srv = sdg.Server()
+    rep.barrier()
     t_start = time.perf_counter()
     ids = []
     for r, f, g in zip(reqs, fields, gaps):
@@ -498,19 +552,28 @@ def run_served(args):
     st = srv.stats()
     srv.close()
     total = float(sum(work))
-    line = {"metric": "DOF-updates/s per RHS eval", "value": total / makespan,
-            "unit": "DOF-updates/s per RHS eval", "n_gpus": 1, "steps": len(reqs),
+    value = rep.rate(total, makespan)
+    makespan = rep.max(makespan)
+    p50 = rep.max(np.percentile(tts, 50))
+    p99 = rep.max(np.percentile(tts, 99))
+    busy = rep.max(st["busy_s"])
+    busy_rate = rep.sum(st["dof_steps"] * 3) / max(busy, 1e-9)
+    seq_rate = rep.sum(seq_rate)
+    rep.close()
+    if rank != 0:
+        return
+    line = {"metric": "DOF-updates/s per RHS eval", "value": value,
+            "unit": "DOF-updates/s per RHS eval", "n_gpus": world, "steps": len(reqs),
             "warmup": 0, "ms_per_step": 1e3 * makespan / len(reqs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": "served", "requests": len(reqs),
                        "arrival_rate_per_s": lam, "load": 0.8,
-                       "ne_per_axis": "U{8..32}", "p": "U{3..11}", "nstep": "U{50..400}"},
-            "served": {"p50_tts_s": float(np.percentile(tts, 50)),
-                       "p99_tts_s": float(np.percentile(tts, 99)),
+                       "ne_per_axis": "U{8..32}", "p": "U{3..11}", "nstep": "U{50..400}",
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "served": {"p50_tts_s": p50, "p99_tts_s": p99,
                        "mean_tts_s": float(tts.mean()), "makespan_s": makespan,
-                       "device_busy_s": st["busy_s"],
-                       "throughput_busy": st["dof_steps"] * 3 / max(st["busy_s"], 1e-9),
+                       "device_busy_s": busy, "throughput_busy": busy_rate,
                        "one_at_a_time_fp64": seq_rate, "one_at_a_time_sample": n_seq}}
     print(json.dumps(line), flush=True)
 

@@ -20,11 +20,14 @@ constexpr int NQ = SDG_NQ;
 
 // Launches a persistent pipelined kernel: attribute and occupancy set-up on
 // the first call of each instantiation (a call with no tiles only primes
-// it, e.g. before a stream capture), then one block per resident slot.
-template <bool BATCH, typename K, typename Args, typename Dm>
-int launch_pipe(K kern, size_t smem, int ntiles, const LaunchSpec& s, const Args& a,
-                const Dm& d) {
-  static int blocks_per_sm = 0;  // per instantiation; the plan is fixed
+// it, e.g. before a stream capture), then one block per resident slot.  The
+// kernel is a template argument so that the set-up state belongs to that
+// kernel: kernels of one signature (tendency and stage forms) differ in
+// their shared-memory plans.
+template <auto KERN, typename Args, typename Dm>
+int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, const Dm& d) {
+  constexpr auto kern = KERN;
+  static int blocks_per_sm = 0;  // per kernel; its plan is fixed
   if (blocks_per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
@@ -82,10 +85,10 @@ int run(const LaunchSpec& s) {
     const int ntiles =
         batch ? s.batch_ntiles : (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
     if (batch)
-      return launch_pipe<true>(tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, true>,
-                               P::BYTES, ntiles, s, a, d);
-    return launch_pipe<false>(tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false>,
-                              P::BYTES, ntiles, s, a, d);
+      return launch_pipe<tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, true>>(
+          P::BYTES, ntiles, s, a, d);
+    return launch_pipe<tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false>>(
+        P::BYTES, ntiles, s, a, d);
   }
 
   const size_t smem = SmemLayout<NQ, TC>::BYTES;
