@@ -59,8 +59,10 @@ struct Ops {
   int nq = 0;
   std::vector<double> D;      // row-major D(i,l)
   std::vector<double> lift;   // Lift_mat(Np,6)
-  double* lift64 = nullptr;
-  float* lift32 = nullptr;
+  double* lift64 = nullptr;   // verbatim (exact kernels)
+  double* lift64f = nullptr;  // factored when Lift_mat factorises (fast kernels)
+  float* lift32 = nullptr;    // the fast table in FP32 (mixed kernels)
+  std::vector<double> lift_z; // z-face factors (2, Nq); empty: not factored
 };
 
 enum InstState { kQueued = 0, kRunning = 1, kDone = 2, kFailed = 3 };
@@ -180,6 +182,7 @@ struct Ensemble {
     }
     for (auto& o : ops) {
       if (o.second->lift64) cudaFree(o.second->lift64);
+      if (o.second->lift64f) cudaFree(o.second->lift64f);
       if (o.second->lift32) cudaFree(o.second->lift32);
     }
     if (status) cudaFree(status);
@@ -228,11 +231,16 @@ struct Ensemble {
     for (int i = 0; i < nq; ++i)
       for (int l = 0; l < nq; ++l) o->D[i * nq + l] = D1D[i + nq * l];
     o->lift.assign(Lift, Lift + 6L * np);
+    std::vector<double> fact;
+    if (!lift_factor(Lift, nq, &fact, &o->lift_z)) fact.clear();
+    const double* fast = fact.empty() ? Lift : fact.data();
     std::vector<float> l32(6L * np);
-    for (long x = 0; x < 6L * np; ++x) l32[x] = static_cast<float>(Lift[x]);
+    for (long x = 0; x < 6L * np; ++x) l32[x] = static_cast<float>(fast[x]);
     ENS_CUDA(cudaMalloc(&o->lift64, 6L * np * sizeof(double)));
+    ENS_CUDA(cudaMalloc(&o->lift64f, 6L * np * sizeof(double)));
     ENS_CUDA(cudaMalloc(&o->lift32, 6L * np * sizeof(float)));
     ENS_CUDA(cudaMemcpy(o->lift64, Lift, 6L * np * sizeof(double), cudaMemcpyHostToDevice));
+    ENS_CUDA(cudaMemcpy(o->lift64f, fast, 6L * np * sizeof(double), cudaMemcpyHostToDevice));
     ENS_CUDA(cudaMemcpy(o->lift32, l32.data(), 6L * np * sizeof(float),
                         cudaMemcpyHostToDevice));
     *out = o.get();
@@ -253,9 +261,12 @@ struct Ensemble {
     g->flags = mixed ? 0 : flags;
     g->ops = o;
     g->epb = pipe_elems_per_tile(nq);
+    // The fast pipelined kernels need the factored lift.
+    const bool exact = !mixed && (flags & SDG_FLAG_EXACT);
     const bool can_pipe = pipe_supported(nq, mixed ? kStageMixed2 : kStageF64) &&
                           pipe_supported(nq, mixed ? kStageMixed1 : kStageF64) &&
-                          pipe_supported(nq, mixed ? kStageMixed3 : kStageF64);
+                          pipe_supported(nq, mixed ? kStageMixed3 : kStageF64) &&
+                          (exact || !o->lift_z.empty());
     g->variant = can_pipe ? kVariantPipe : kVariantBlock;
     ENS_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     ENS_CUDA(cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming));
@@ -403,8 +414,11 @@ struct Ensemble {
     l.kind = g->mixed ? (kStageMixed1 + st) : kStageF64;
     l.exact = (g->flags & SDG_FLAG_EXACT) != 0;
     l.order = (g->flags & SDG_FLAG_ORDER_GENERAL) ? kOrderGeneral : kOrderOpt1;
-    l.lift = g->mixed ? static_cast<const void*>(g->ops->lift32) : g->ops->lift64;
+    l.lift = g->mixed  ? static_cast<const void*>(g->ops->lift32)
+             : l.exact ? g->ops->lift64
+                       : g->ops->lift64f;
     l.D = g->ops->D.data();
+    l.lift_z = g->ops->lift_z.empty() ? nullptr : g->ops->lift_z.data();
     l.stream = s;
     l.variant = g->variant;
     l.status = status;

@@ -190,6 +190,9 @@ struct sdg_handle {
   bool primed = false;
   cudaStream_t stream = nullptr;
   std::vector<double> D;  // row-major D(i,l)
+  // z-face factors of the factored lift (2, Nq); empty when Lift_mat has no
+  // tensor-product factorisation (the fast kernels then read it verbatim).
+  std::vector<double> lift_z;
 
   // Compressed tables (device).
   double* lift64 = nullptr;
@@ -267,6 +270,7 @@ LaunchSpec base_spec(const sdg_handle* h, bool f32) {
   s.elem0 = 0;
   s.nelem = h->Ne;
   s.D = h->D.data();
+  s.lift_z = h->lift_z.empty() ? nullptr : h->lift_z.data();
   s.stream = h->stream;
   s.variant = h->variant;
   s.status = h->status;
@@ -573,7 +577,13 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
 
   std::vector<int> hs(NhaloNode);
   for (int b = 0; b < NhaloNode; ++b) hs[b] = halo_src_map[b] - 1;
-  if ((rc = upload(&h->lift64, Lift_mat, 6L * Np)) ||
+  // The exact FP64 kernels read the verbatim Lift_mat; the fast ones (FP64
+  // and mixed) read its tensor-product factorisation when the table has one.
+  std::vector<double> lift_fact;
+  if (!lift_factor(Lift_mat, Nq, &lift_fact, &h->lift_z)) lift_fact.clear();
+  const double* lift_fast = lift_fact.empty() ? Lift_mat : lift_fact.data();
+  const double* lift_f64 = (flags & SDG_FLAG_EXACT) ? Lift_mat : lift_fast;
+  if ((rc = upload(&h->lift64, lift_f64, 6L * Np)) ||
       (rc = upload(&h->pb_halo, pbh.data(), pbh.size())) ||
       (rc = upload(&h->pb_direct, pbd.data(), pbd.size())) ||
       (rc = upload(&h->esc64, esc.data(), esc.size())) ||
@@ -582,7 +592,7 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
     return bail(rc);
   {
     std::vector<float> l32(6L * Np), e32(esc.size()), f32v(fsc.size());
-    for (size_t i = 0; i < l32.size(); ++i) l32[i] = static_cast<float>(Lift_mat[i]);
+    for (size_t i = 0; i < l32.size(); ++i) l32[i] = static_cast<float>(lift_fast[i]);
     for (size_t i = 0; i < e32.size(); ++i) e32[i] = static_cast<float>(esc[i]);
     for (size_t i = 0; i < f32v.size(); ++i) f32v[i] = static_cast<float>(fsc[i]);
     if ((rc = upload(&h->lift32, l32.data(), l32.size())) ||

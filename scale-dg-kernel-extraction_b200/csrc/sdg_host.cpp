@@ -58,6 +58,34 @@ int face_node(int Nq, int f, int fp) {
   }
 }
 
+bool lift_factor(const double* Lift, int Nq, std::vector<double>* expanded,
+                 std::vector<double>* lift_z) {
+  const long Nq2 = static_cast<long>(Nq) * Nq, Np = Nq2 * Nq;
+  expanded->clear();
+  lift_z->clear();
+  double mx = 0.0;
+  for (long x = 0; x < 6 * Np; ++x) mx = std::fmax(mx, std::fabs(Lift[x]));
+  std::vector<double> ex(6 * Np);
+  const long stride[3] = {1, Nq, Nq2};  // node offset of one step along i, j, k
+  double spread = 0.0;
+  for (int f = 0; f < 6; ++f)
+    for (long n = 0; n < Np; ++n) {
+      const long ijk[3] = {n % Nq, (n / Nq) % Nq, n / Nq2};
+      const int ax = kFaceAxis[f];
+      const double ref = Lift[Np * f + ijk[ax] * stride[ax]];  // tangential (0, 0)
+      ex[Np * f + n] = ref;
+      spread = std::fmax(spread, std::fabs(Lift[Np * f + n] - ref));
+    }
+  if (!(spread <= kLiftFactorTol * mx)) return false;
+  lift_z->resize(2L * Nq);
+  for (int k = 0; k < Nq; ++k) {
+    (*lift_z)[k] = ex[Np * 4 + Nq2 * k];
+    (*lift_z)[Nq + k] = ex[Np * 5 + Nq2 * k];
+  }
+  expanded->swap(ex);
+  return true;
+}
+
 }  // namespace sdg
 
 using namespace sdg;

@@ -40,6 +40,10 @@ struct LaunchSpec {
   int nelem;
   double rk_a, rk_b, dt;
   const double* D;     // row-major D(i,l), NQ*NQ
+  // Factored lift of the fast kernels: the z-face factors lz(k, f) for
+  // f = -z, +z ((2, NQ), host memory), given when `lift` holds the
+  // tensor-product factorisation of Lift_mat; null for the verbatim table.
+  const double* lift_z;
   cudaStream_t stream;
   int variant;         // KernelVariant
   int* status;         // device status word (bounded-wait timeouts)

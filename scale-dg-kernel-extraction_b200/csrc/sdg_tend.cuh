@@ -125,6 +125,7 @@ struct SmemLayout {
 template <int NQ, typename TC>
 struct DMat {
   TC d[NQ * NQ];
+  TC lz[2 * NQ];  // z-face lift factors (-z, +z) of the factored fast lift
 };
 
 // Sum_{l} A(l)*B(l) in the reference's order (see header comment).

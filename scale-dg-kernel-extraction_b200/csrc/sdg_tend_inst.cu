@@ -71,13 +71,17 @@ int run(const LaunchSpec& s) {
   a.ntiles = s.batch_ntiles;
   DMat<NQ, TC> d;
   for (int i = 0; i < NQ * NQ; ++i) d.d[i] = static_cast<TC>(s.D[i]);
+  for (int i = 0; i < 2 * NQ; ++i)
+    d.lz[i] = s.lift_z ? static_cast<TC>(s.lift_z[i]) : TC(0);
   using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
   auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
   const bool batch = s.batch_tiles != nullptr;
-  // Batched arrays are allocated 256-byte aligned by the batch itself.
-  const bool can_pipe = P::BYTES <= kPipeMaxSmem &&
+  // Batched arrays are allocated 256-byte aligned by the batch itself.  The
+  // fast pipelined kernels need the factored lift; with a verbatim table a
+  // fast launch takes the one-tile-per-block kernel.
+  const bool can_pipe = P::BYTES <= kPipeMaxSmem && (EXACT || s.lift_z != nullptr) &&
                         (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
-                                   aligned(s.w) && (!STAGE || aligned(s.q0))));
+                                   aligned(s.w) && aligned(s.escale) && aligned(s.fscale)));
   if (batch && !can_pipe) return static_cast<int>(cudaErrorNotSupported);
   const bool pipe =
       batch || ((s.variant == kVariantPipe || s.variant == kVariantAuto) && can_pipe);

@@ -2,30 +2,38 @@
 // kernel (same arithmetic as tend_kernel in sdg_tend.cuh, same results).
 //
 // Each block loops over tiles of EPB consecutive elements.  The element data
-// a tile needs (q, u, v, w and, for RK stages 2-3, q0) are contiguous in
-// HBM, so one elected thread moves them into a shared-memory ring of NSTAGE
-// tiles with cp.async.bulk (the TMA bulk-copy engine), completing on an
-// mbarrier per ring slot.  A slot stays resident for its whole tile (the
-// epilogue re-reads q and q0 from it instead of holding them in registers)
-// and is refilled, with the tile NSTAGE iterations on, as the block starts
-// the next tile.  Compute threads never stall on their own element loads:
-// the bytes in flight per SM are set by the ring, not by occupancy.  The
-// plus-side face values (in neighbouring elements) are gathered with
-// ordinary loads issued before the ring wait, so their latency overlaps it.
+// a tile needs (q, u, v, w and the tile's rows of escale and fscale) are
+// contiguous in HBM, so one elected thread moves them into a shared-memory
+// ring of NSTAGE tiles with cp.async.bulk (the TMA bulk-copy engine),
+// completing on an mbarrier per ring slot.  A slot stays resident for its
+// whole tile and is refilled, with the tile NSTAGE iterations on, as the
+// block starts the next tile.  Compute threads never stall on their own
+// element loads: the bytes in flight per SM are set by the ring, not by
+// occupancy.
 //
-// Thread mapping.  Column (a,b) of an element (its z-line) is owned by H
-// threads.  With H = 2 (Nq^2 a multiple of 32, i.e. p = 7 and p = 15) the two
-// owners sit in different warps, so the half index h is warp-uniform:
-//   h = 0: nodes k < Nq/2, the x-line (j,k) = (a,b), faces 1-2 at node
-//          (a,b), the -z face;
-//   h = 1: nodes k >= Nq/2, the y-line (i,k) = (a,b), faces 3-4, the +z face.
-// The two halves of a z-column meet in shared memory for the z-derivative.
-// With H = 1 one thread plays every role, as in tend_kernel.  Splitting
-// halves the registers per thread and doubles the warps per SM for the same
-// shared memory; each output's summation chain is unchanged.
+// Loads that are not contiguous per tile are issued early, as ordinary
+// loads whose latency later work covers: the plus-side face values in
+// neighbouring elements (from a face-neighbour row loaded before the ring
+// wait) are issued before the line contractions, and the face fluxes come
+// after them; for RK stages 2-3, the column's q0 values, which a bulk
+// prefetch issued with the tile's ring copies has brought into L2, are
+// loaded before the face fluxes and used in the epilogue.
 //
-// For p <= 7 each thread keeps the lift coefficients of its column nodes in
-// registers for the whole persistent loop.
+// Shared memory per block: the ring, plus one area of (q, un) pairs for the
+// minus side of the four x/y faces.  The x- and y-line buffers of the
+// derivative reuse the current slot's u and v regions: those are dead once
+// every thread holds its column, so a barrier separates the column reads
+// from the line-buffer writes.  At p = 7 this keeps an FP64 block at 73 KB,
+// three blocks (12 warps) per SM.
+//
+// Thread mapping, as in tend_kernel: thread t = a + Nq*b of an element owns
+// the z-column (a,b) in registers (z-derivative, z faces, combine), the
+// x-line (j,k) = (a,b) and y-line (i,k) = (a,b), and node t of each x/y face.
+//
+// Lift.  The fast kernels use the tensor-product factorisation of Lift_mat
+// (the host checks it against the table): four per-thread factors and the
+// z-face factors from the parameter bank.  The exact kernels read the
+// verbatim table through the read-only path.
 //
 // Every wait is bounded.  A wait that runs out sets *status and the block
 // drains its own copies (again bounded) and returns; the host reports the
@@ -42,6 +50,9 @@ constexpr unsigned kWaitSpins = 1u << 22;
 // Largest shared-memory plan the pipelined kernel is used with: two blocks
 // of it fit on one SM (228 KB).
 constexpr size_t kPipeMaxSmem = 110 * 1024;
+// Shared memory of one SM and the per-block reservation of the driver.
+constexpr size_t kSmemPerSM = 228 * 1024;
+constexpr size_t kSmemPerBlockReserved = 1024;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -93,16 +104,24 @@ __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Thread geometry of the pipelined kernel.
-// kSplitColumns enables the two-owners-per-column mapping (H = 2) where
-// Nq^2 is a multiple of 32.  Measured on B200 at p = 7 it doubles the warps
-// per SM but is slower (60.9 vs 70.6 G DOF-updates/s FP64): the kernel is
-// limited by the shared-memory pipe, and the split adds 15% wavefronts and
-// barrier stalls.  Kept for experiments; off by default.
-#ifndef SDG_SPLIT_COLUMNS
-#define SDG_SPLIT_COLUMNS 0
-#endif
-constexpr bool kSplitColumns = SDG_SPLIT_COLUMNS != 0;
+// Bulk prefetch of a global range into L2 (TMA engine); addr and bytes are
+// multiples of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes)
+               : "memory");
+}
+
+// Orders this thread's shared-memory writes before later bulk copies (async
+// proxy) into the same bytes.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Streaming load (read once: evict-first in the caches).
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+  return __ldcs(p);
+}
 
 // Placement of node (i,j,k) in the x-line and y-line buffers.  Generic
 // orders use the padded layout of tend_kernel.  For Nq = 8 an XOR swizzle
@@ -146,22 +165,15 @@ struct Pair2<float> {
   using type = float2;
 };
 
+// Thread geometry: Nq^2 threads per element, EPB elements per block
+// (128 threads where Nq^2 divides it).
 template <int NQ>
 struct PipeGeo {
   static constexpr int NQ2 = NQ * NQ;
   static constexpr int NP = NQ2 * NQ;
-  static constexpr int H = (kSplitColumns && NQ2 % 32 == 0) ? 2 : 1;  // owners per column
-  static constexpr int KH = NQ / H;                  // column nodes per thread
-  static constexpr int TPE = H * NQ2;                // threads per element
-  static constexpr int TARGET = (H == 2) ? 256 : 128;
-  static constexpr int EPB = TPE >= TARGET ? 1 : TARGET / TPE;
-  static constexpr int THREADS = EPB * TPE;
+  static constexpr int EPB = NQ2 >= 128 ? 1 : 128 / NQ2;
+  static constexpr int THREADS = EPB * NQ2;
   static constexpr int SBUF = LineIdx<NQ>::SIZE;
-  // Per-element work area (in compute-type words): x- and y-line buffers,
-  // the four x/y faces' (q_minus, un_minus) pairs (each face flux
-  // overwrites its q_minus), the two z-face fluxes and, when H = 2, the
-  // z-column exchange buffer.
-  static constexpr int WORK_ELEM = 2 * SBUF + 8 * NQ2 + 2 * NQ2 + (H == 2 ? NP : 0);
 };
 
 // Shared-memory plan of the pipelined kernel.
@@ -172,18 +184,36 @@ struct PipePlan {
   static constexpr int NP = G::NP;
   static constexpr int NSTAGE = 2;
   static constexpr size_t r16(size_t x) { return (x + 15) & ~size_t(15); }
+  static constexpr size_t mx(size_t a, size_t b) { return a > b ? a : b; }
   // Each array region holds EPB elements plus 32 bytes of slack: the source
   // range is widened to 16-byte boundaries at both ends (at most 12 bytes
-  // each for 4- and 8-byte elements).
+  // each for 4- and 8-byte elements).  The u and v regions double as the
+  // x- and y-line buffers once the tile's columns are in registers.
   static constexpr size_t QB = r16(sizeof(TQ) * EPB * NP + 32);
-  static constexpr size_t VB = r16(sizeof(TV) * EPB * NP + 32);
-  static constexpr size_t Q0B = STAGE ? r16(sizeof(double) * EPB * NP + 32) : 0;
-  static constexpr size_t SLOT = QB + 3 * VB + Q0B;
-  static constexpr size_t WORK = r16(sizeof(TC) * G::WORK_ELEM * EPB);
+  static constexpr size_t VB =
+      mx(r16(sizeof(TV) * EPB * NP + 32), r16(sizeof(TC) * EPB * G::SBUF));
+  static constexpr size_t EB = r16(sizeof(TC) * 3 * EPB + 32);  // escale rows
+  static constexpr size_t FB = r16(sizeof(TC) * 6 * EPB + 32);  // fscale rows
+  static constexpr size_t OFF_U = QB;
+  static constexpr size_t OFF_V = QB + VB;
+  static constexpr size_t OFF_W = QB + 2 * VB;
+  static constexpr size_t OFF_E = QB + 3 * VB;
+  static constexpr size_t OFF_F = OFF_E + EB;
+  static constexpr size_t SLOT = OFF_F + FB;
+  // (q, un) pairs of the four x/y faces' minus side, per element.
+  static constexpr size_t FACE = r16(sizeof(TC) * 8 * G::NQ2 * EPB);
   static constexpr size_t BARS = 16 * NSTAGE;
-  static constexpr size_t BYTES = NSTAGE * SLOT + WORK + BARS;
-  // Lift coefficients kept in registers when the column is short.
-  static constexpr bool LIFT_REGS = NQ <= 8;
+  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + BARS;
+  // Blocks per SM that the shared memory allows (the register budget per
+  // thread follows from it), at most 4.
+  static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
+      kSmemPerSM / (BYTES + kSmemPerBlockReserved) > 4
+          ? 4
+          : (kSmemPerSM / (BYTES + kSmemPerBlockReserved) < 1
+                 ? 1
+                 : kSmemPerSM / (BYTES + kSmemPerBlockReserved)));
+  static constexpr int MIN_BLOCKS =
+      (BLOCKS_PER_SM_SMEM * G::THREADS > 512) ? 512 / G::THREADS : BLOCKS_PER_SM_SMEM;
 };
 
 // Arrays and element range of one tile.
@@ -200,14 +230,14 @@ struct TileCtx {
   const TC* fscale;
   double dt;
   int e0;  // first element (index into the arrays)
-  int n;   // elements in the tile (1..EPB)
+  int n;   // elements in the tile (0..EPB; 0 past the last tile)
 };
 
 // BATCH is a compile-time property of the kernel, so a single-instance
 // launch keeps its pointers in the parameter bank instead of registers.
 template <int EPB, bool BATCH, typename TQ, typename TV, typename TO, typename TC>
 __device__ __forceinline__ TileCtx<TQ, TV, TO, TC> tile_ctx(const TendArgs<TQ, TV, TO, TC>& A,
-                                                            int tile) {
+                                                            int tile, int ntiles) {
   TileCtx<TQ, TV, TO, TC> c;
   if constexpr (!BATCH) {
     c.q = A.q;
@@ -221,9 +251,9 @@ __device__ __forceinline__ TileCtx<TQ, TV, TO, TC> tile_ctx(const TendArgs<TQ, T
     c.fscale = A.fscale;
     c.dt = A.dt;
     c.e0 = A.elem0 + tile * EPB;
-    c.n = min(EPB, A.nelem - tile * EPB);
+    c.n = tile < ntiles ? min(EPB, A.nelem - tile * EPB) : 0;
   } else {
-    const BatchTile t = A.tiles[tile];
+    const BatchTile t = A.tiles[tile < ntiles ? tile : 0];
     const BatchInst& I = A.insts[t.inst];
     c.q = static_cast<const TQ*>(I.q);
     c.u = static_cast<const TV*>(I.u);
@@ -236,7 +266,7 @@ __device__ __forceinline__ TileCtx<TQ, TV, TO, TC> tile_ctx(const TendArgs<TQ, T
     c.fscale = static_cast<const TC*>(I.fscale);
     c.dt = I.dt;
     c.e0 = t.e0;
-    c.n = t.n;
+    c.n = tile < ntiles ? t.n : 0;
   }
   return c;
 }
@@ -256,133 +286,94 @@ __device__ __forceinline__ int opp_offset(int f, int a, int b) {
   }
 }
 
-// Phase 4 of one thread: z-derivative, lift, combine and store for the
-// column nodes k = K0 .. K0+KH-1 (K0 compile-time, so D's rows are
-// immediate constant-bank operands).
-template <int NQ, int K0, int KH, int ORDER, bool STAGE, bool LIFT_REGS, bool EXACT,
-          typename TQ, typename TV, typename TO, typename TC>
-__device__ __forceinline__ void column_epilogue(
-    const TendArgs<TQ, TV, TO, TC>& A, const DMat<NQ, TC>& D,
-    const TileCtx<TQ, TV, TO, TC>& C, int e, long base, int t, int a, int b, const TC* zcol,
-    const TC* sX, const TC* sY, const TC* fQ, TC f5, TC f6, const TQ* sq,
-    const double* sq0, const TC* lreg) {
-  constexpr int NQ2 = NQ * NQ;
-  constexpr int NP = NQ2 * NQ;
-  using LI = LineIdx<NQ>;
-  using AR = Ar<TC, EXACT>;
-  const TC* es = C.escale + 3 * static_cast<long>(e);
-  const TC e1 = es[0], e2 = es[1], e3 = es[2];
-#pragma unroll
-  for (int kk = 0; kk < KH; ++kk) {
-    const int k = K0 + kk;
-    const TC dz = contract<NQ, ORDER, AR, TC>([&](int l) { return zcol[l]; },
-                                              [&](int l) { return D.d[k * NQ + l]; });
-    TC L[6];
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      if constexpr (LIFT_REGS) L[f] = lreg[6 * kk + f];
-      else L[f] = ldro(A.lift + t + NQ2 * k + NP * f);
-    }
-    // x/y face fluxes sit at stride 2 (the .x of each (q, un) pair).
-    TC lf = AR::mul(L[0], fQ[2 * (0 * NQ2 + a + NQ * k)]);
-    lf = AR::mad(L[1], fQ[2 * (1 * NQ2 + b + NQ * k)], lf);
-    lf = AR::mad(L[2], fQ[2 * (2 * NQ2 + a + NQ * k)], lf);
-    lf = AR::mad(L[3], fQ[2 * (3 * NQ2 + b + NQ * k)], lf);
-    lf = AR::mad(L[4], f5, lf);
-    lf = AR::mad(L[5], f6, lf);
-    TC acc = AR::mul(e1, sX[LI::x(a, b, k)]);
-    acc = AR::mad(e2, sY[LI::y(a, b, k)], acc);
-    acc = AR::mad(e3, dz, acc);
-    acc = AR::add(acc, lf);
-    const TC dqdt = -acc;
-    const long n = base + t + NQ2 * k;
-    if constexpr (!STAGE) {
-      C.out[n] = static_cast<TO>(dqdt);
-    } else {
-      using AD = Ar<double, EXACT>;
-      double qd;
-      // The stage input at its stored precision, from the tile's ring slot.
-      qd = static_cast<double>(sq[t + NQ2 * k]);
-      double r = AD::mul(A.rk_b, AD::mad(C.dt, static_cast<double>(dqdt), qd));
-      // q0 is read from the tile's ring slot (still resident in phase 4).
-      if (A.rk_a != 0.0) r = AD::mad(A.rk_a, sq0[t + NQ2 * k], r);
-      C.out[n] = static_cast<TO>(r);
-    }
-  }
+// Byte range of elements [e0, e0+n) in an array of `per_elem` bytes per
+// element, widened to 16-byte boundaries: start, length and the offset of
+// element e0 inside the copied range.
+__device__ __forceinline__ void tile_range(int e0, int n, size_t per_elem, size_t* lo16,
+                                           uint32_t* bytes, uint32_t* shift) {
+  const size_t lo = static_cast<size_t>(e0) * per_elem;
+  const size_t hi = static_cast<size_t>(e0 + n) * per_elem;
+  *lo16 = lo & ~size_t(15);
+  *bytes = static_cast<uint32_t>(((hi + 15) & ~size_t(15)) - *lo16);
+  *shift = static_cast<uint32_t>(lo - *lo16);
 }
 
+__device__ __forceinline__ uint32_t tile_shift(int e0, size_t per_elem) {
+  return static_cast<uint32_t>((static_cast<size_t>(e0) * per_elem) & 15);
+}
+
+// Blocks per SM the kernel is compiled for: what its shared memory allows,
+// but at most 2 for the exact kernels, whose separately rounded arithmetic
+// needs the larger register budget.
+template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE>
+constexpr int pipe_min_blocks() {
+  constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE>::MIN_BLOCKS;
+  return (EXACT && m > 2) ? 2 : m;
+}
+
+// The thread bound is the block size rounded up to whole warps (the
+// compiler front end of CUDA 12.9 fails on this kernel with a bound of,
+// e.g., 81 threads at Nq = 9).
 template <int NQ, typename TQ, typename TV, typename TO, typename TC, bool EXACT,
           int ORDER, bool STAGE, bool BATCH>
-__global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
+__global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
+                                  (pipe_min_blocks<NQ, TQ, TV, TC, EXACT, STAGE>()))
     tend_pipe_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
                      const __grid_constant__ DMat<NQ, TC> D) {
   using G = PipeGeo<NQ>;
   using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
   using AR = Ar<TC, EXACT>;
   using Ctx = TileCtx<TQ, TV, TO, TC>;
+  using V2 = typename Pair2<TC>::type;
+  using LI = LineIdx<NQ>;
   constexpr int NQ2 = G::NQ2;
   constexpr int NP = G::NP;
   constexpr int EPB = G::EPB;
-  constexpr int H = G::H;
-  constexpr int KH = G::KH;
   constexpr int NS = P::NSTAGE;
-  constexpr int NFACE = 4 / H;   // x/y faces evaluated per thread
-  constexpr int NZF = 2 / H;     // z faces evaluated per thread
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* slots = smem_raw;
-  TC* work = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::WORK);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::FACE);
 
-  const int s = threadIdx.x / G::TPE;            // element slot
-  const int r = threadIdx.x - s * G::TPE;
-  const int h = (H == 2) ? r / NQ2 : 0;          // warp-uniform half
-  const int t = r - h * NQ2;                     // column index a + NQ*b
+  const int s = threadIdx.x / NQ2;               // element slot of the tile
+  const int t = threadIdx.x - s * NQ2;           // column index a + NQ*b
   const int a = t % NQ;
   const int b = t / NQ;
-  const int k0 = h * KH;
   const int ntiles = BATCH ? A.ntiles : (A.nelem + EPB - 1) / EPB;
 
-  using V2 = typename Pair2<TC>::type;
-  using LI = LineIdx<NQ>;
-  TC* sX = work + s * G::WORK_ELEM;
-  TC* sY = sX + G::SBUF;
   // [4][NQ2] (q, un) of the minus side; phase 2 overwrites q with the flux,
   // so the lift reads the x/y face fluxes at stride 2 from fQ.
-  V2* fM = reinterpret_cast<V2*>(sY + G::SBUF);
-  TC* fQ = sY + G::SBUF;
-  TC* fZ = fQ + 8 * NQ2;       // [2][NQ2] z-face fluxes
-  TC* sZ = fZ + 2 * NQ2;       // [NQ][NQ2] z-column exchange (H = 2)
-
-  // Byte range of elements [e0, e0+n) in an array of element size `sz`,
-  // widened to 16-byte boundaries.
-  auto range = [&](int e0, int n, size_t sz, size_t* lo16, uint32_t* bytes,
-                   uint32_t* shift) {
-    const size_t lo = static_cast<size_t>(e0) * NP * sz;
-    const size_t hi = static_cast<size_t>(e0 + n) * NP * sz;
-    *lo16 = lo & ~size_t(15);
-    *bytes = static_cast<uint32_t>(((hi + 15) & ~size_t(15)) - *lo16);
-    *shift = static_cast<uint32_t>(lo - *lo16);
-  };
+  V2* fM = reinterpret_cast<V2*>(smem_raw + NS * P::SLOT) + s * 4 * NQ2;
+  TC* fQ = reinterpret_cast<TC*>(fM);
 
   // Producer: one thread fills ring slot `slot` with tile `tile`.
   auto issue = [&](int tile, int slot) {
-    const Ctx c = tile_ctx<EPB, BATCH>(A, tile);
+    const Ctx c = tile_ctx<EPB, BATCH>(A, tile, ntiles);
     unsigned char* base = slots + slot * P::SLOT;
-    const void* src[5] = {c.q, c.u, c.v, c.w, c.q0};
-    const size_t sz[5] = {sizeof(TQ), sizeof(TV), sizeof(TV), sizeof(TV), sizeof(double)};
-    const size_t off[5] = {0, P::QB, P::QB + P::VB, P::QB + 2 * P::VB, P::QB + 3 * P::VB};
-    const int narr = (STAGE && A.rk_a != 0.0) ? 5 : 4;
-    size_t lo[5];
-    uint32_t by[5], sh[5], total = 0;
-    for (int k = 0; k < narr; ++k) {
-      range(c.e0, c.n, sz[k], &lo[k], &by[k], &sh[k]);
+    const void* src[6] = {c.q, c.u, c.v, c.w, c.escale, c.fscale};
+    const size_t per[6] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
+                           sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6};
+    const size_t off[6] = {0, P::OFF_U, P::OFF_V, P::OFF_W, P::OFF_E, P::OFF_F};
+    size_t lo[6];
+    uint32_t by[6], sh[6], total = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      tile_range(c.e0, c.n, per[k], &lo[k], &by[k], &sh[k]);
       total += by[k];
     }
     mbar_arrive_expect_tx(&bars[slot], total);
-    for (int k = 0; k < narr; ++k)
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
       bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
                &bars[slot]);
+    // q0 (RK stages 2-3) is read by the epilogue straight from global
+    // memory; bring the tile's range into L2 now.
+    if (STAGE && A.rk_a != 0.0) {
+      size_t l0;
+      uint32_t b0, s0;
+      tile_range(c.e0, c.n, sizeof(double) * NP, &l0, &b0, &s0);
+      bulk_prefetch_l2(reinterpret_cast<const unsigned char*>(c.q0) + l0, b0);
+    }
   };
 
   if (threadIdx.x == 0) {
@@ -396,15 +387,13 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
       if (tile < ntiles) issue(tile, k);
     }
 
-  // Lift coefficients of this thread's column nodes, kept for the loop.
-  constexpr int LR = P::LIFT_REGS ? 6 * KH : 1;
-  TC lreg[LR];
-  if constexpr (P::LIFT_REGS) {
+  // Factored lift of the fast kernels, kept for the loop: entry (a, b, 0, f)
+  // of the factored table is l_f(b) for the y faces and l_f(a) for the x
+  // faces.  The exact kernels read the verbatim table in the epilogue.
+  TC lreg[4];
+  if constexpr (!EXACT) {
 #pragma unroll
-    for (int kk = 0; kk < KH; ++kk)
-#pragma unroll
-      for (int f = 0; f < 6; ++f)
-        lreg[6 * kk + f] = ldro(A.lift + t + NQ2 * (k0 + kk) + NP * f);
+    for (int f = 0; f < 4; ++f) lreg[f] = ldro(A.lift + t + NP * f);
   }
 
   for (int it = 0;; ++it) {
@@ -412,34 +401,15 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
     if (tile >= ntiles) break;
     const int slot = it % NS;
     const uint32_t parity = (it / NS) & 1;
-    const Ctx C = tile_ctx<EPB, BATCH>(A, tile);
+    const Ctx C = tile_ctx<EPB, BATCH>(A, tile, ntiles);
     const bool active = s < C.n;
     const int e = C.e0 + (active ? s : 0);
     const long base = static_cast<long>(e) * NP;
 
-    // ---- Plus-side face gathers, issued before the ring wait -------------
-    TC qP[NFACE], unP[NFACE], qZ[NZF], wZ[NZF];
-    if (active) {
-      const int* pb = C.pbase + 6 * static_cast<long>(e);
+    // The element's face-neighbour row, needed after phase 1.
+    int pbc[6];
 #pragma unroll
-      for (int ff = 0; ff < NFACE; ++ff) {
-        const int f = h * NFACE + ff;
-        const int p = pb[f];
-        const long idx = (p >= 0) ? static_cast<long>(p) + opp_offset<NQ>(f, a, b)
-                                  : static_cast<long>(-1 - p) + t;
-        qP[ff] = static_cast<TC>(ldro(C.q + idx));
-        unP[ff] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx) : ldro(C.v + idx));
-      }
-#pragma unroll
-      for (int zz = 0; zz < NZF; ++zz) {
-        const int f = 4 + h * NZF + zz;
-        const int p = pb[f];
-        const long idx = (p >= 0) ? static_cast<long>(p) + opp_offset<NQ>(f, a, b)
-                                  : static_cast<long>(-1 - p) + t;
-        qZ[zz] = static_cast<TC>(ldro(C.q + idx));
-        wZ[zz] = static_cast<TC>(ldro(C.w + idx));
-      }
-    }
+    for (int f = 0; f < 6; ++f) pbc[f] = active ? ldro(C.pbase + 6 * static_cast<long>(e) + f) : 0;
 
     // ---- Wait for the tile's slot (bounded, block-uniform) -----------------
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity));
@@ -465,104 +435,167 @@ __global__ void __launch_bounds__(PipeGeo<NQ>::THREADS, 2)
       if (nt < ntiles) issue(nt, (it - 1) % NS);
     }
 
-    // ---- Phase 1: read this thread's column nodes out of the slot ---------
     unsigned char* sb = slots + slot * P::SLOT;
-    size_t lo;
-    uint32_t by, shq, shv;
-    range(C.e0, C.n, sizeof(TQ), &lo, &by, &shq);
-    range(C.e0, C.n, sizeof(TV), &lo, &by, &shv);
-    const TQ* sq = reinterpret_cast<const TQ*>(sb + shq) + s * NP;
-    const TV* su = reinterpret_cast<const TV*>(sb + P::QB + shv) + s * NP;
-    const TV* sv = reinterpret_cast<const TV*>(sb + P::QB + P::VB + shv) + s * NP;
-    const TV* sw = reinterpret_cast<const TV*>(sb + P::QB + 2 * P::VB + shv) + s * NP;
-    uint32_t sh0 = 0;
-    if constexpr (STAGE) range(C.e0, C.n, sizeof(double), &lo, &by, &sh0);
-    const double* sq0 =
-        reinterpret_cast<const double*>(sb + P::QB + 3 * P::VB + sh0) + s * NP;
+    const TQ* sq =
+        reinterpret_cast<const TQ*>(sb + tile_shift(C.e0, sizeof(TQ) * NP)) + s * NP;
+    const uint32_t shv = tile_shift(C.e0, sizeof(TV) * NP);
+    const TV* su = reinterpret_cast<const TV*>(sb + P::OFF_U + shv) + s * NP;
+    const TV* sv = reinterpret_cast<const TV*>(sb + P::OFF_V + shv) + s * NP;
+    const TV* sw = reinterpret_cast<const TV*>(sb + P::OFF_W + shv) + s * NP;
+    const TC* ses =
+        reinterpret_cast<const TC*>(sb + P::OFF_E + tile_shift(C.e0, sizeof(TC) * 3)) + 3 * s;
+    const TC* sfs =
+        reinterpret_cast<const TC*>(sb + P::OFF_F + tile_shift(C.e0, sizeof(TC) * 6)) + 6 * s;
+    // z-flux column in place of w.
+    static_assert(sizeof(TV) == sizeof(TC), "w and q*w share their slots");
+    TC* sz = reinterpret_cast<TC*>(sb + P::OFF_W + shv) + s * NP;
+    // Line buffers in the u and v regions (valid after the column reads).
+    TC* sX = reinterpret_cast<TC*>(sb + P::OFF_U) + s * G::SBUF;
+    TC* sY = reinterpret_cast<TC*>(sb + P::OFF_V) + s * G::SBUF;
 
-    TC fz[KH];
-    TC qlo = TC(0), qhi = TC(0);   // q on the -z and +z faces
-    TC wM[NZF];
+    // ---- Phase 1: the column's volume fluxes and minus-side face values ---
+    // q*w replaces w in place: each thread reads and writes only its own
+    // column there, so the z-flux column waits in shared memory for phase 4.
+    TC fx[NQ], fy[NQ];
+    TC wlo = TC(0), whi = TC(0);
     if (active) {
 #pragma unroll
-      for (int kk = 0; kk < KH; ++kk) {
-        const int k = k0 + kk;
+      for (int k = 0; k < NQ; ++k) {
         const int n = t + NQ2 * k;
         const TC qv = static_cast<TC>(sq[n]);
         const TC uv = static_cast<TC>(su[n]);
         const TC vv = static_cast<TC>(sv[n]);
         const TC wv = static_cast<TC>(sw[n]);
-        if (kk == 0) qlo = qv;
-        if (kk == KH - 1) qhi = qv;
-        sX[LI::x(a, b, k)] = AR::mul(qv, uv);
-        sY[LI::y(a, b, k)] = AR::mul(qv, vv);
-        fz[kk] = AR::mul(qv, wv);
-        if constexpr (H == 2) sZ[t + NQ2 * k] = fz[kk];
-        if (kk == 0 && k == 0) wM[0] = wv;                 // -z face (k = 1)
-        if (kk == KH - 1 && k == NQ - 1) wM[NZF - 1] = wv;  // +z face (k = Nq)
+        if (k == 0) wlo = wv;
+        if (k == NQ - 1) whi = wv;
+        fx[k] = AR::mul(qv, uv);
+        fy[k] = AR::mul(qv, vv);
+        sz[n] = AR::mul(qv, wv);
         if (b == 0) fM[0 * NQ2 + a + NQ * k] = V2{qv, vv};
         if (a == NQ - 1) fM[1 * NQ2 + b + NQ * k] = V2{qv, uv};
         if (b == NQ - 1) fM[2 * NQ2 + a + NQ * k] = V2{qv, vv};
         if (a == 0) fM[3 * NQ2 + b + NQ * k] = V2{qv, uv};
       }
     }
+    __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        sX[LI::x(a, b, k)] = fx[k];
+        sY[LI::y(a, b, k)] = fy[k];
+      }
+    }
     __syncthreads();
 
+    // ---- Loads whose latency phase 3 covers --------------------------------
+    // Plus-side face values of the x/y faces (face node t) and z faces.
+    TC qP[4], unP[4], qZ[2], wZ[2];
     if (active) {
-      // ---- Phase 2: face fluxes -------------------------------------------
-      const TC* fs = C.fscale + 6 * static_cast<long>(e);
 #pragma unroll
-      for (int ff = 0; ff < NFACE; ++ff) {
-        const int f = h * NFACE + ff;
+      for (int f = 0; f < 4; ++f) {
+        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
+                                       : static_cast<long>(-1 - pbc[f]) + t;
+        qP[f] = static_cast<TC>(ldro(C.q + idx));
+        unP[f] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx) : ldro(C.v + idx));
+      }
+#pragma unroll
+      for (int z = 0; z < 2; ++z) {
+        const int f = 4 + z;
+        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
+                                       : static_cast<long>(-1 - pbc[f]) + t;
+        qZ[z] = static_cast<TC>(ldro(C.q + idx));
+        wZ[z] = static_cast<TC>(ldro(C.w + idx));
+      }
+    }
+    constexpr int NQ0 = STAGE ? NQ : 1;
+    double q0r[NQ0];
+    const bool use_q0 = STAGE && A.rk_a != 0.0;
+    TC f5 = TC(0), f6 = TC(0);
+    if (active) {
+      // ---- Phase 3: x-line and y-line contractions, in place --------------
+      TC line[NQ];
+#pragma unroll
+      for (int l = 0; l < NQ; ++l) line[l] = sX[LI::x(l, a, b)];
+#pragma unroll
+      for (int i = 0; i < NQ; ++i)
+        sX[LI::x(i, a, b)] = contract<NQ, ORDER, AR, TC>(
+            [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+#pragma unroll
+      for (int l = 0; l < NQ; ++l) line[l] = sY[LI::y(a, l, b)];
+#pragma unroll
+      for (int j = 0; j < NQ; ++j)
+        sY[LI::y(a, j, b)] = contract<NQ, ORDER, AR, TC>(
+            [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+      // The line buffers live in the slot that the next refill overwrites.
+      fence_proxy_async_smem();
+      // q0 of the column (RK stages 2-3), in L2 since the tile's copies were
+      // issued.
+      if constexpr (STAGE) {
+        if (use_q0) {
+#pragma unroll
+          for (int k = 0; k < NQ; ++k) q0r[k] = ld_stream(C.q0 + base + t + NQ2 * k);
+        }
+      }
+      // ---- Phase 2: face fluxes -------------------------------------------
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
         const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
         const V2 m = fM[f * NQ2 + t];
-        fQ[2 * (f * NQ2 + t)] = upwind_flux<AR, TC>(m.x, m.y, qP[ff], unP[ff], sg, fs[f]);
+        fQ[2 * (f * NQ2 + t)] = upwind_flux<AR, TC>(m.x, m.y, qP[f], unP[f], sg, sfs[f]);
       }
-#pragma unroll
-      for (int zz = 0; zz < NZF; ++zz) {
-        const int f = 4 + h * NZF + zz;   // 4: -z (k = 1), 5: +z (k = Nq)
-        const TC qm = (f == 4) ? qlo : qhi;
-        fZ[(f - 4) * NQ2 + t] =
-            upwind_flux<AR, TC>(qm, wM[zz], qZ[zz], wZ[zz], f == 4 ? TC(-1) : TC(1), fs[f]);
-      }
-      // ---- Phase 3: line contractions (x-line for h = 0, y-line for h = 1)
-      TC line[NQ];
-      if (H == 1 || h == 0) {
-#pragma unroll
-        for (int l = 0; l < NQ; ++l) line[l] = sX[LI::x(l, a, b)];
-#pragma unroll
-        for (int i = 0; i < NQ; ++i)
-          sX[LI::x(i, a, b)] = contract<NQ, ORDER, AR, TC>(
-              [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
-      }
-      if (H == 1 || h == 1) {
-#pragma unroll
-        for (int l = 0; l < NQ; ++l) line[l] = sY[LI::y(a, l, b)];
-#pragma unroll
-        for (int j = 0; j < NQ; ++j)
-          sY[LI::y(a, j, b)] = contract<NQ, ORDER, AR, TC>(
-              [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
-      }
+      const TC qlo = static_cast<TC>(sq[t]), qhi = static_cast<TC>(sq[t + NQ2 * (NQ - 1)]);
+      f5 = upwind_flux<AR, TC>(qlo, wlo, qZ[0], wZ[0], TC(-1), sfs[4]);
+      f6 = upwind_flux<AR, TC>(qhi, whi, qZ[1], wZ[1], TC(1), sfs[5]);
     }
     __syncthreads();
 
     if (active) {
       // ---- Phase 4: z-derivative, lift, combine, store ---------------------
-      TC zcol[NQ];
-      if constexpr (H == 2) {
+      const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
+      TC fz[NQ];
 #pragma unroll
-        for (int l = 0; l < NQ; ++l) zcol[l] = sZ[t + NQ2 * l];
-      } else {
+      for (int l = 0; l < NQ; ++l) fz[l] = sz[t + NQ2 * l];
 #pragma unroll
-        for (int l = 0; l < NQ; ++l) zcol[l] = fz[l];
+      for (int k = 0; k < NQ; ++k) {
+        const TC dz = contract<NQ, ORDER, AR, TC>([&](int l) { return fz[l]; },
+                                                  [&](int l) { return D.d[k * NQ + l]; });
+        TC L[6];
+        if constexpr (!EXACT) {
+#pragma unroll
+          for (int f = 0; f < 4; ++f) L[f] = lreg[f];
+          L[4] = D.lz[k];
+          L[5] = D.lz[NQ + k];
+        } else {
+#pragma unroll
+          for (int f = 0; f < 6; ++f) L[f] = ldro(A.lift + t + NQ2 * k + NP * f);
+        }
+        // tensorprod_Lift_hexahedral (kern:278-283): face order 1..6; the
+        // x/y face fluxes sit at stride 2 (the .x of each (q, un) pair).
+        TC lf = AR::mul(L[0], fQ[2 * (0 * NQ2 + a + NQ * k)]);
+        lf = AR::mad(L[1], fQ[2 * (1 * NQ2 + b + NQ * k)], lf);
+        lf = AR::mad(L[2], fQ[2 * (2 * NQ2 + a + NQ * k)], lf);
+        lf = AR::mad(L[3], fQ[2 * (3 * NQ2 + b + NQ * k)], lf);
+        lf = AR::mad(L[4], f5, lf);
+        lf = AR::mad(L[5], f6, lf);
+        // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
+        TC acc = AR::mul(e1, sX[LI::x(a, b, k)]);
+        acc = AR::mad(e2, sY[LI::y(a, b, k)], acc);
+        acc = AR::mad(e3, dz, acc);
+        acc = AR::add(acc, lf);
+        const TC dqdt = -acc;
+        const long n = base + t + NQ2 * k;
+        if constexpr (!STAGE) {
+          C.out[n] = static_cast<TO>(dqdt);
+        } else {
+          // q = rk_a*q0 + rk_b*(q + dt*dqdt), main.f90:70-71, in FP64, with
+          // the stage input at its stored precision from the ring slot.
+          using AD = Ar<double, EXACT>;
+          const double qd = static_cast<double>(sq[t + NQ2 * k]);
+          double r = AD::mul(A.rk_b, AD::mad(C.dt, static_cast<double>(dqdt), qd));
+          if (use_q0) r = AD::mad(A.rk_a, q0r[k], r);
+          C.out[n] = static_cast<TO>(r);
+        }
       }
-      const TC f5 = fZ[t], f6 = fZ[NQ2 + t];
-      if (H == 1 || h == 0)
-        column_epilogue<NQ, 0, KH, ORDER, STAGE, P::LIFT_REGS, EXACT>(
-            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, sq, sq0, lreg);
-      else
-        column_epilogue<NQ, (H == 2 ? KH : 0), KH, ORDER, STAGE, P::LIFT_REGS, EXACT>(
-            A, D, C, e, base, t, a, b, zcol, sX, sY, fQ, f5, f6, sq, sq0, lreg);
     }
   }
 }
