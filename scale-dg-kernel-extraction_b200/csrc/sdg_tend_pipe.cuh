@@ -31,9 +31,9 @@
 // x-line (j,k) = (a,b) and y-line (i,k) = (a,b), and node t of each x/y face.
 //
 // Lift.  The fast kernels use the tensor-product factorisation of Lift_mat
-// (the host checks it against the table): four per-thread factors and the
-// z-face factors from the parameter bank.  The exact kernels read the
-// verbatim table through the read-only path.
+// (the host checks it against the table): the x/y-face factors from a small
+// shared table and the z-face factors from the parameter bank.  The exact
+// kernels read the verbatim table through the read-only path.
 //
 // Every wait is bounded.  A wait that runs out sets *status and the block
 // drains its own copies (again bounded) and returns; the host reports the
@@ -123,34 +123,52 @@ __device__ __forceinline__ T ld_stream(const T* p) {
   return __ldcs(p);
 }
 
-// Placement of node (i,j,k) in the x-line and y-line buffers.  Generic
-// orders use the padded layout of tend_kernel.  For Nq = 8 an XOR swizzle
-// over the 16 eight-byte bank pairs makes every access pattern of the
-// kernel conflict-free: column (i fastest, two j per half-warp), x-line
-// (fixed i, j and two k per half-warp) and y-line (fixed j, i and two k):
+// Placement of node (i,j,k) in the x-line and y-line buffers.  A thread
+// (a,b) touches them in three patterns: its column (a,b,k) for k = 0..Nq-1,
+// its x-line (l,a,b) and its y-line (a,l,b) for l = 0..Nq-1.  Each pattern
+// has a per-thread base and a compile-time step, so the unrolled accesses
+// are one register plus immediates:
+//   column   x: colx(a,b,k&1) + CS*k     y: coly(a,b,k&1) + CS*k
+//   x-line   xl(xl_base(a,b), l)         y-line  yl(yl_base(a,b), l)
+// Generic orders use the padded layout of tend_kernel (row stride RS,
+// plane stride PS).  For Nq = 8 an XOR swizzle over the 16 eight-byte bank
+// pairs makes every pattern conflict-free (column: i fastest, two j per
+// half-warp; x-line: fixed i, j and two k per half-warp; y-line: fixed j,
+// i and two k):
 //   x(i,j,k) = 16*((j + 8k) >> 1) + ((i ^ j) & 7) + 8*((j + k) & 1)
 //   y(i,j,k) = 16*((i + 8k) >> 1) + ((i ^ j) & 7) + 8*((i + k) & 1)
-// (bijections onto 0..511).  The padded layout costs two wavefronts more
-// per column access.
+// (bijections onto 0..511).  Both line patterns then reduce to
+// x(l,a,b) = y(a,l,b) = (64b + 16(a>>1) + 8((a+b)&1) + a) ^ l, the low three
+// bits of the bracket before "+ a" being zero.  The padded layout costs two
+// wavefronts more per column access.
 template <int NQ>
 struct LineIdx {
   static constexpr int SIZE = Geo<NQ>::SBUF;
-  static __device__ __forceinline__ int x(int i, int j, int k) {
-    return i + Geo<NQ>::RS * j + Geo<NQ>::PS * k;
-  }
-  static __device__ __forceinline__ int y(int i, int j, int k) {
-    return i + Geo<NQ>::RS * j + Geo<NQ>::PS * k;
-  }
+  static constexpr int RS = Geo<NQ>::RS;
+  static constexpr int CS = Geo<NQ>::PS;
+  static __device__ __forceinline__ int colx(int a, int b, int) { return a + RS * b; }
+  static __device__ __forceinline__ int coly(int a, int b, int) { return a + RS * b; }
+  static __device__ __forceinline__ int xl_base(int a, int b) { return RS * a + CS * b; }
+  static __device__ __forceinline__ int xl(int base, int l) { return base + l; }
+  static __device__ __forceinline__ int yl_base(int a, int b) { return a + CS * b; }
+  static __device__ __forceinline__ int yl(int base, int l) { return base + RS * l; }
 };
 template <>
 struct LineIdx<8> {
   static constexpr int SIZE = 512;
-  static __device__ __forceinline__ int x(int i, int j, int k) {
-    return 16 * ((j + 8 * k) >> 1) + ((i ^ j) & 7) + 8 * ((j + k) & 1);
+  static constexpr int CS = 64;
+  static __device__ __forceinline__ int colx(int a, int b, int par) {
+    return 16 * (b >> 1) + ((a ^ b) & 7) + 8 * ((b + par) & 1);
   }
-  static __device__ __forceinline__ int y(int i, int j, int k) {
-    return 16 * ((i + 8 * k) >> 1) + ((i ^ j) & 7) + 8 * ((i + k) & 1);
+  static __device__ __forceinline__ int coly(int a, int b, int par) {
+    return 16 * (a >> 1) + ((a ^ b) & 7) + 8 * ((a + par) & 1);
   }
+  static __device__ __forceinline__ int xl_base(int a, int b) {
+    return (64 * b + 16 * (a >> 1) + 8 * ((a + b) & 1)) | a;
+  }
+  static __device__ __forceinline__ int xl(int base, int l) { return base ^ l; }
+  static __device__ __forceinline__ int yl_base(int a, int b) { return xl_base(a, b); }
+  static __device__ __forceinline__ int yl(int base, int l) { return base ^ l; }
 };
 
 // A (q_minus, un_minus) pair of a face node, stored in one 8- or 16-byte word.
@@ -202,8 +220,10 @@ struct PipePlan {
   static constexpr size_t SLOT = OFF_F + FB;
   // (q, un) pairs of the four x/y faces' minus side, per element.
   static constexpr size_t FACE = r16(sizeof(TC) * 8 * G::NQ2 * EPB);
+  // Per-face lift factors l_f(n) of the fast kernels, (4, Nq).
+  static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
   static constexpr size_t BARS = 16 * NSTAGE;
-  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + BARS;
+  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + LIFTB + BARS;
   // Blocks per SM that the shared memory allows (the register budget per
   // thread follows from it), at most 4.
   static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
@@ -333,7 +353,9 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* slots = smem_raw;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::FACE);
+  TC* sL = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::FACE);
+  uint64_t* bars =
+      reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::FACE + P::LIFTB);
 
   const int s = threadIdx.x / NQ2;               // element slot of the tile
   const int t = threadIdx.x - s * NQ2;           // column index a + NQ*b
@@ -380,21 +402,21 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     for (int k = 0; k < NS; ++k) mbar_init(&bars[k], 1);
     fence_barrier_init();
   }
+  // Factored lift of the fast kernels: l_f(n) is the factored table's entry
+  // at normal index n, tangential indices 0 (faces 1, 3 lie along j, faces
+  // 2, 4 along i).  The exact kernels read the verbatim table instead.
+  if constexpr (!EXACT) {
+    for (int x = threadIdx.x; x < 4 * NQ; x += blockDim.x) {
+      const int f = x / NQ, n = x - f * NQ;
+      sL[x] = ldro(A.lift + NP * f + ((f & 1) ? n : NQ * n));
+    }
+  }
   __syncthreads();
   if (threadIdx.x == 0)
     for (int k = 0; k < NS; ++k) {
       const int tile = blockIdx.x + k * gridDim.x;
       if (tile < ntiles) issue(tile, k);
     }
-
-  // Factored lift of the fast kernels, kept for the loop: entry (a, b, 0, f)
-  // of the factored table is l_f(b) for the y faces and l_f(a) for the x
-  // faces.  The exact kernels read the verbatim table in the epilogue.
-  TC lreg[4];
-  if constexpr (!EXACT) {
-#pragma unroll
-    for (int f = 0; f < 4; ++f) lreg[f] = ldro(A.lift + t + NP * f);
-  }
 
   for (int it = 0;; ++it) {
     const int tile = blockIdx.x + it * gridDim.x;
@@ -459,6 +481,12 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     TC fx[NQ], fy[NQ];
     TC wlo = TC(0), whi = TC(0);
     if (active) {
+      // A thread on an x face (a = 0 or Nq-1) stores its (q, u) there, one on
+      // a y face (b = 0 or Nq-1) its (q, v): faces -x/+x are 4/2, -y/+y 1/3.
+      const bool onx = (a == 0) || (a == NQ - 1);
+      const bool ony = (b == 0) || (b == NQ - 1);
+      V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
+      V2* fmy = fM + (b == 0 ? 0 : 2) * NQ2 + a;
 #pragma unroll
       for (int k = 0; k < NQ; ++k) {
         const int n = t + NQ2 * k;
@@ -471,18 +499,18 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         fx[k] = AR::mul(qv, uv);
         fy[k] = AR::mul(qv, vv);
         sz[n] = AR::mul(qv, wv);
-        if (b == 0) fM[0 * NQ2 + a + NQ * k] = V2{qv, vv};
-        if (a == NQ - 1) fM[1 * NQ2 + b + NQ * k] = V2{qv, uv};
-        if (b == NQ - 1) fM[2 * NQ2 + a + NQ * k] = V2{qv, vv};
-        if (a == 0) fM[3 * NQ2 + b + NQ * k] = V2{qv, uv};
+        if (onx) fmx[NQ * k] = V2{qv, uv};
+        if (ony) fmy[NQ * k] = V2{qv, vv};
       }
     }
     __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
     if (active) {
+      TC* cx[2] = {sX + LI::colx(a, b, 0), sX + LI::colx(a, b, 1)};
+      TC* cy[2] = {sY + LI::coly(a, b, 0), sY + LI::coly(a, b, 1)};
 #pragma unroll
       for (int k = 0; k < NQ; ++k) {
-        sX[LI::x(a, b, k)] = fx[k];
-        sY[LI::y(a, b, k)] = fy[k];
+        cx[k & 1][LI::CS * k] = fx[k];
+        cy[k & 1][LI::CS * k] = fy[k];
       }
     }
     __syncthreads();
@@ -514,17 +542,18 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     if (active) {
       // ---- Phase 3: x-line and y-line contractions, in place --------------
       TC line[NQ];
+      const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
 #pragma unroll
-      for (int l = 0; l < NQ; ++l) line[l] = sX[LI::x(l, a, b)];
+      for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
 #pragma unroll
       for (int i = 0; i < NQ; ++i)
-        sX[LI::x(i, a, b)] = contract<NQ, ORDER, AR, TC>(
+        sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
             [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
 #pragma unroll
-      for (int l = 0; l < NQ; ++l) line[l] = sY[LI::y(a, l, b)];
+      for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
 #pragma unroll
       for (int j = 0; j < NQ; ++j)
-        sY[LI::y(a, j, b)] = contract<NQ, ORDER, AR, TC>(
+        sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, TC>(
             [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
       // The line buffers live in the slot that the next refill overwrites.
       fence_proxy_async_smem();
@@ -552,6 +581,15 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     if (active) {
       // ---- Phase 4: z-derivative, lift, combine, store ---------------------
       const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
+      const TC* cx[2] = {sX + LI::colx(a, b, 0), sX + LI::colx(a, b, 1)};
+      const TC* cy[2] = {sY + LI::coly(a, b, 0), sY + LI::coly(a, b, 1)};
+      TC lxy[4];
+      if constexpr (!EXACT) {
+        lxy[0] = sL[b];
+        lxy[1] = sL[NQ + a];
+        lxy[2] = sL[2 * NQ + b];
+        lxy[3] = sL[3 * NQ + a];
+      }
       TC fz[NQ];
 #pragma unroll
       for (int l = 0; l < NQ; ++l) fz[l] = sz[t + NQ2 * l];
@@ -562,7 +600,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         TC L[6];
         if constexpr (!EXACT) {
 #pragma unroll
-          for (int f = 0; f < 4; ++f) L[f] = lreg[f];
+          for (int f = 0; f < 4; ++f) L[f] = lxy[f];
           L[4] = D.lz[k];
           L[5] = D.lz[NQ + k];
         } else {
@@ -578,8 +616,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         lf = AR::mad(L[4], f5, lf);
         lf = AR::mad(L[5], f6, lf);
         // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
-        TC acc = AR::mul(e1, sX[LI::x(a, b, k)]);
-        acc = AR::mad(e2, sY[LI::y(a, b, k)], acc);
+        TC acc = AR::mul(e1, cx[k & 1][LI::CS * k]);
+        acc = AR::mad(e2, cy[k & 1][LI::CS * k], acc);
         acc = AR::mad(e3, dz, acc);
         acc = AR::add(acc, lf);
         const TC dqdt = -acc;
