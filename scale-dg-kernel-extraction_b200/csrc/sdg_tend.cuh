@@ -151,6 +151,46 @@ __device__ __forceinline__ T contract(FA A, FB B) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core line contractions (fast FP64 kernels, Nq = 8)
+// ---------------------------------------------------------------------------
+// The x- and y-derivatives of an element are the 8x8-by-8x64 products
+// D * F_x and D * F_y (over the 64 lines of each direction).  The fast FP64
+// kernels at Nq = 8 compute them with mma.sync m8n8k4 (DMMA): one 8x8 output
+// tile = one k-plane of the element, two chained k-steps (l = 0..3, then
+// 4..7).  A DMMA does 256 FMAs in one warp instruction where the DFMA form
+// needs 32 per instruction, at the same FP64 peak.  Fragments (PTX ISA,
+// m8n8k4 .f64): lane L holds A(L>>2, L&3), B(L&3, L>>2) and
+// C(L>>2, 2(L&3) + {0,1}).  Every kernel variant uses this same sequence,
+// so their fast FP64 results stay bit-identical.
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b,
+                                            double c0, double c1) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};"
+      : "=d"(d0), "=d"(d1)
+      : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+// This lane's A fragments of D for the two k-steps: D(L>>2, 4s + (L&3)).
+template <typename DM>
+__device__ __forceinline__ void dmma_dfrag(const DM& D, double* a0, double* a1) {
+  const int lane = threadIdx.x & 31;
+  *a0 = D.d[(lane >> 2) * 8 + (lane & 3)];
+  *a1 = D.d[(lane >> 2) * 8 + 4 + (lane & 3)];
+}
+
+// The kernels that contract x- and y-lines on the tensor cores.
+template <int NQ, typename TC, bool EXACT>
+constexpr bool kTensorLines = (NQ == 8) && !EXACT && sizeof(TC) == 8;
+
+// One 8x8 output tile: d = D * B, with this lane's B fragments b0 = B(L&3,
+// L>>2) and b1 = B(4 + (L&3), L>>2).
+__device__ __forceinline__ void dmma_tile8(double a0, double a1, double b0, double b1,
+                                           double* d0, double* d1) {
+  double c0, c1;
+  dmma_m8n8k4(c0, c1, a0, b0, 0.0, 0.0);
+  dmma_m8n8k4(*d0, *d1, a1, b1, c0, c1);
+}
+
 __device__ __forceinline__ double absv(double x) { return fabs(x); }
 __device__ __forceinline__ float absv(float x) { return fabsf(x); }
 
@@ -334,7 +374,28 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
       f6 = upwind_flux<AR, TC>(qc[NQ - 1], whi, q6, w6, TC(1), fs[5]);
     }
     // ---- Phase 3: x-line and y-line contractions, in place --------------
-    {
+    if constexpr (kTensorLines<NQ, TC, EXACT>) {
+      // DMMA tiles: the element's two warps take four k-planes each; a
+      // plane is read and rewritten only by its warp.
+      double a0, a1;
+      dmma_dfrag(D, &a0, &a1);
+      const int lane = threadIdx.x & 31, g = lane >> 2, qd = lane & 3;
+      const int we = (t >> 5);  // warp of the element
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const int T = 4 * we + kk;
+        double d0, d1;
+        // x: B(l, j) = F_x(i = l, j, k = T); C(i, j) = DxF(i, j, T).
+        dmma_tile8(a0, a1, sX[qd + RS * g + PS * T], sX[4 + qd + RS * g + PS * T], &d0, &d1);
+        sX[g + RS * (2 * qd) + PS * T] = d0;
+        sX[g + RS * (2 * qd + 1) + PS * T] = d1;
+        // y: B(l, i) = F_y(i, j = l, k = T); C(j, i) = DyF(i, j, T).
+        dmma_tile8(a0, a1, sY[g + RS * qd + PS * T], sY[g + RS * (4 + qd) + PS * T], &d0,
+                   &d1);
+        sY[2 * qd + RS * g + PS * T] = d0;
+        sY[2 * qd + 1 + RS * g + PS * T] = d1;
+      }
+    } else {
       TC line[NQ];
 #pragma unroll
       for (int l = 0; l < NQ; ++l) line[l] = sX[l + RS * a + PS * b];

@@ -171,6 +171,22 @@ struct LineIdx<8> {
   static __device__ __forceinline__ int yl(int base, int l) { return base ^ l; }
 };
 
+// Line buffers of the tensor-core contractions (fast FP64, Nq = 8): eight
+// k-planes of 64, each an 8x8 (i,j) block in which
+//   x:  F_x(i,j) at px(i,j) = (j ^ h(i)) + 8i,  DxF(i,j) at qx(i,j) = (j ^ (i&6)) + 8i
+//   y:  F_y(i,j) at py(i,j) = (i ^ h(j)) + 8j,  DyF(i,j) at qy(i,j) = (i ^ (j&6)) + 8j
+// with h(n) = ((n&2) << 1) | ((n&4) >> 1).  The four patterns on each buffer
+// (column writes of F, B-fragment loads, 16-byte C-fragment stores, column
+// reads of the result) each put a half-warp's eight-byte accesses on 16
+// distinct bank pairs.
+struct TensorIdx8 {
+  static __device__ __forceinline__ int h(int n) { return ((n & 2) << 1) | ((n & 4) >> 1); }
+  static __device__ __forceinline__ int px(int i, int j) { return (j ^ h(i)) + 8 * i; }
+  static __device__ __forceinline__ int qx(int i, int j) { return (j ^ (i & 6)) + 8 * i; }
+  static __device__ __forceinline__ int py(int i, int j) { return (i ^ h(j)) + 8 * j; }
+  static __device__ __forceinline__ int qy(int i, int j) { return (i ^ (j & 6)) + 8 * j; }
+};
+
 // A (q_minus, un_minus) pair of a face node, stored in one 8- or 16-byte word.
 template <typename T>
 struct Pair2;
@@ -350,6 +366,10 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
   constexpr int NP = G::NP;
   constexpr int EPB = G::EPB;
   constexpr int NS = P::NSTAGE;
+  // x/y line contractions on the tensor cores (fast FP64, Nq = 8).
+  constexpr bool TENSOR = kTensorLines<NQ, TC, EXACT>;
+  double da0 = 0.0, da1 = 0.0;  // this lane's A fragments of D
+  if constexpr (TENSOR) dmma_dfrag(D, &da0, &da1);
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* slots = smem_raw;
@@ -505,12 +525,22 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     }
     __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
     if (active) {
-      TC* cx[2] = {sX + LI::colx(a, b, 0), sX + LI::colx(a, b, 1)};
-      TC* cy[2] = {sY + LI::coly(a, b, 0), sY + LI::coly(a, b, 1)};
+      if constexpr (TENSOR) {
+        TC* px = sX + TensorIdx8::px(a, b);
+        TC* py = sY + TensorIdx8::py(a, b);
 #pragma unroll
-      for (int k = 0; k < NQ; ++k) {
-        cx[k & 1][LI::CS * k] = fx[k];
-        cy[k & 1][LI::CS * k] = fy[k];
+        for (int k = 0; k < NQ; ++k) {
+          px[NQ2 * k] = fx[k];
+          py[NQ2 * k] = fy[k];
+        }
+      } else {
+        TC* cx[2] = {sX + LI::colx(a, b, 0), sX + LI::colx(a, b, 1)};
+        TC* cy[2] = {sY + LI::coly(a, b, 0), sY + LI::coly(a, b, 1)};
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) {
+          cx[k & 1][LI::CS * k] = fx[k];
+          cy[k & 1][LI::CS * k] = fy[k];
+        }
       }
     }
     __syncthreads();
@@ -541,20 +571,40 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     TC f5 = TC(0), f6 = TC(0);
     if (active) {
       // ---- Phase 3: x-line and y-line contractions, in place --------------
-      TC line[NQ];
-      const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
+      if constexpr (TENSOR) {
+        // DMMA tiles: the element's two warps take four k-planes each; a
+        // plane is read and rewritten only by its warp.
+        const int lane = threadIdx.x & 31, g = lane >> 2, qd = lane & 3;
+        const int we = t >> 5;  // warp of the element
+        using TI = TensorIdx8;
 #pragma unroll
-      for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
+        for (int kk = 0; kk < 4; ++kk) {
+          TC* px = sX + NQ2 * (4 * we + kk);
+          TC* py = sY + NQ2 * (4 * we + kk);
+          double d0, d1;
+          // x: B(l, j) = F_x(l, j), C(i, j) = DxF(i, j) on this plane.
+          dmma_tile8(da0, da1, px[TI::px(qd, g)], px[TI::px(4 + qd, g)], &d0, &d1);
+          *reinterpret_cast<double2*>(px + TI::qx(g, 2 * qd)) = make_double2(d0, d1);
+          // y: B(l, i) = F_y(i, l), C(j, i) = DyF(i, j).
+          dmma_tile8(da0, da1, py[TI::py(g, qd)], py[TI::py(g, 4 + qd)], &d0, &d1);
+          *reinterpret_cast<double2*>(py + TI::qy(2 * qd, g)) = make_double2(d0, d1);
+        }
+      } else {
+        TC line[NQ];
+        const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
 #pragma unroll
-      for (int i = 0; i < NQ; ++i)
-        sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
-            [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+        for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
 #pragma unroll
-      for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
+        for (int i = 0; i < NQ; ++i)
+          sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
+              [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
 #pragma unroll
-      for (int j = 0; j < NQ; ++j)
-        sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, TC>(
-            [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+        for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
+#pragma unroll
+        for (int j = 0; j < NQ; ++j)
+          sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, TC>(
+              [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+      }
       // The line buffers live in the slot that the next refill overwrites.
       fence_proxy_async_smem();
       // q0 of the column (RK stages 2-3), in L2 since the tile's copies were
@@ -581,8 +631,20 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     if (active) {
       // ---- Phase 4: z-derivative, lift, combine, store ---------------------
       const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
-      const TC* cx[2] = {sX + LI::colx(a, b, 0), sX + LI::colx(a, b, 1)};
-      const TC* cy[2] = {sY + LI::coly(a, b, 0), sY + LI::coly(a, b, 1)};
+      // This column's entries of the x/y results: k-plane k, then the
+      // layout's in-plane offset.
+      const TC* cx[2];
+      const TC* cy[2];
+      if constexpr (TENSOR) {
+        cx[0] = cx[1] = sX + TensorIdx8::qx(a, b);
+        cy[0] = cy[1] = sY + TensorIdx8::qy(a, b);
+      } else {
+        cx[0] = sX + LI::colx(a, b, 0);
+        cx[1] = sX + LI::colx(a, b, 1);
+        cy[0] = sY + LI::coly(a, b, 0);
+        cy[1] = sY + LI::coly(a, b, 1);
+      }
+      constexpr int CS = TENSOR ? NQ2 : LI::CS;
       TC lxy[4];
       if constexpr (!EXACT) {
         lxy[0] = sL[b];
@@ -616,8 +678,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         lf = AR::mad(L[4], f5, lf);
         lf = AR::mad(L[5], f6, lf);
         // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
-        TC acc = AR::mul(e1, cx[k & 1][LI::CS * k]);
-        acc = AR::mad(e2, cy[k & 1][LI::CS * k], acc);
+        TC acc = AR::mul(e1, cx[k & 1][CS * k]);
+        acc = AR::mad(e2, cy[k & 1][CS * k], acc);
         acc = AR::mad(e3, dz, acc);
         acc = AR::add(acc, lf);
         const TC dqdt = -acc;
