@@ -19,8 +19,8 @@
 // prefetch issued with the tile's ring copies has brought into L2, are
 // loaded before the face fluxes and used in the epilogue.
 //
-// Shared memory per block: the ring, plus one area of (q, un) pairs for the
-// minus side of the four x/y faces.  The x- and y-line buffers of the
+// Shared memory per block: the ring, plus one area for the minus side of the
+// four x/y faces and their fluxes (FaceArea).  The x- and y-line buffers of the
 // derivative reuse the current slot's u and v regions: those are dead once
 // every thread holds its column, so a barrier separates the column reads
 // from the line-buffer writes.  At p = 7 this keeps an FP64 block at 73 KB,
@@ -199,6 +199,30 @@ struct Pair2<float> {
   using type = float2;
 };
 
+// Per-element area of minus-side face values and face fluxes (in
+// compute-type words).  x faces (+x = 2, -x = 4): q and u in two arrays,
+// entry (face, k, j) at XOFF*[face is -x] + Nq*k + j, the -x block shifted
+// by Nq^2 + 4 so that the eight writers of one k (a = 0 or Nq-1) hit
+// distinct banks; each x-face flux later replaces its q entry.  y faces
+// (-y = 1, +y = 3): (q, v) pairs, face-major, node a + Nq*k; the pair of
+// -y at node t is later replaced by the (flux -y, flux +y) pair.  Each
+// scalar store of a warp then costs two wavefronts (one per half-warp), and
+// a pair store of the y writers one (they fill one quarter-warp).
+//
+// The split x arrays pay off where a pair is 16 bytes (FP64, whose 128-bit
+// shared accesses run in quarter-warp phases: the x writers span all four).
+// With 8-byte FP32 pairs the x faces keep (q, u) pairs like the y faces
+// (SPLIT = false): face +x at node j + Nq*k, -x at Nq^2 on, and the pair of
+// +x at node t later holds (flux +x, flux -x).
+template <int NQ, bool SPLIT>
+struct FaceArea {
+  static constexpr int NQ2 = NQ * NQ;
+  static constexpr int XOFF = NQ2 + 4;
+  static constexpr int XA = 2 * XOFF;                // one x array (q or u)
+  static constexpr int Y0 = SPLIT ? 2 * XA : 4 * NQ2;  // start of the y pairs
+  static constexpr int ELEM = Y0 + 4 * NQ2;
+};
+
 // Thread geometry: Nq^2 threads per element, EPB elements per block
 // (128 threads where Nq^2 divides it).
 template <int NQ>
@@ -235,7 +259,7 @@ struct PipePlan {
   static constexpr size_t OFF_F = OFF_E + EB;
   static constexpr size_t SLOT = OFF_F + FB;
   // (q, un) pairs of the four x/y faces' minus side, per element.
-  static constexpr size_t FACE = r16(sizeof(TC) * 8 * G::NQ2 * EPB);
+  static constexpr size_t FACE = r16(sizeof(TC) * FaceArea<NQ, sizeof(TC) == 8>::ELEM * EPB);
   // Per-face lift factors l_f(n) of the fast kernels, (4, Nq).
   static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
   static constexpr size_t BARS = 16 * NSTAGE;
@@ -383,10 +407,18 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
   const int b = t / NQ;
   const int ntiles = BATCH ? A.ntiles : (A.nelem + EPB - 1) / EPB;
 
-  // [4][NQ2] (q, un) of the minus side; phase 2 overwrites q with the flux,
-  // so the lift reads the x/y face fluxes at stride 2 from fQ.
-  V2* fM = reinterpret_cast<V2*>(smem_raw + NS * P::SLOT) + s * 4 * NQ2;
-  TC* fQ = reinterpret_cast<TC*>(fM);
+  // Minus-side values of the x/y faces, replaced in phase 2 by the face
+  // fluxes that the epilogue's lift reads (see FaceArea).
+  constexpr bool XSPLIT = sizeof(TC) == 8;
+  using FA = FaceArea<NQ, XSPLIT>;
+  TC* fa = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT) + s * FA::ELEM;
+  TC* xq = fa;                                     // split x faces: q, then the flux
+  TC* xu = fa + FA::XA;                            // split x faces: u
+  V2* ypair = reinterpret_cast<V2*>(fa + FA::Y0);  // y faces: (q, v) pairs
+  // FP32: [4][NQ2] (q, un) pairs of the four faces, face-major; each face
+  // flux replaces the q of its pair, read by the lift at stride 2 (fQ).
+  V2* fM = reinterpret_cast<V2*>(fa);
+  TC* fQ = fa;
 
   // Producer: one thread fills ring slot `slot` with tile `tile`.
   auto issue = [&](int tile, int slot) {
@@ -499,14 +531,15 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     // q*w replaces w in place: each thread reads and writes only its own
     // column there, so the z-flux column waits in shared memory for phase 4.
     TC fx[NQ], fy[NQ];
-    TC wlo = TC(0), whi = TC(0);
+    TC wlo = TC(0), whi = TC(0), qlo = TC(0), qhi = TC(0);
     if (active) {
       // A thread on an x face (a = 0 or Nq-1) stores its (q, u) there, one on
       // a y face (b = 0 or Nq-1) its (q, v): faces -x/+x are 4/2, -y/+y 1/3.
       const bool onx = (a == 0) || (a == NQ - 1);
       const bool ony = (b == 0) || (b == NQ - 1);
+      const int xo = (a == 0 ? FA::XOFF : 0) + b;
       V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
-      V2* fmy = fM + (b == 0 ? 0 : 2) * NQ2 + a;
+      V2* fmy = XSPLIT ? ypair + (b == 0 ? 0 : NQ2) + a : fM + (b == 0 ? 0 : 2) * NQ2 + a;
 #pragma unroll
       for (int k = 0; k < NQ; ++k) {
         const int n = t + NQ2 * k;
@@ -519,7 +552,16 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         fx[k] = AR::mul(qv, uv);
         fy[k] = AR::mul(qv, vv);
         sz[n] = AR::mul(qv, wv);
-        if (onx) fmx[NQ * k] = V2{qv, uv};
+        if constexpr (XSPLIT) {
+          if (k == 0) qlo = qv;
+          if (k == NQ - 1) qhi = qv;
+          if (onx) {
+            xq[xo + NQ * k] = qv;
+            xu[xo + NQ * k] = uv;
+          }
+        } else {
+          if (onx) fmx[NQ * k] = V2{qv, uv};
+        }
         if (ony) fmy[NQ * k] = V2{qv, vv};
       }
     }
@@ -616,13 +658,29 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         }
       }
       // ---- Phase 2: face fluxes -------------------------------------------
+      // Thread t is node t of every x/y face: x node (j,k) = (a,b) at
+      // Nq*b + a of the x arrays, y node (i,k) = (a,b) at t of the pairs.
+      if constexpr (XSPLIT) {
+        const int xn = NQ * b + a;
+        const V2 m1 = ypair[t], m3 = ypair[NQ2 + t];
+        const TC f1 = upwind_flux<AR, TC>(m1.x, m1.y, qP[0], unP[0], TC(-1), sfs[0]);
+        const TC f3 = upwind_flux<AR, TC>(m3.x, m3.y, qP[2], unP[2], TC(1), sfs[2]);
+        const TC f2 = upwind_flux<AR, TC>(xq[xn], xu[xn], qP[1], unP[1], TC(1), sfs[1]);
+        const TC f4 = upwind_flux<AR, TC>(xq[FA::XOFF + xn], xu[FA::XOFF + xn], qP[3],
+                                          unP[3], TC(-1), sfs[3]);
+        xq[xn] = f2;
+        xq[FA::XOFF + xn] = f4;
+        ypair[t] = V2{f1, f3};
+      } else {
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
-        const V2 m = fM[f * NQ2 + t];
-        fQ[2 * (f * NQ2 + t)] = upwind_flux<AR, TC>(m.x, m.y, qP[f], unP[f], sg, sfs[f]);
+        for (int f = 0; f < 4; ++f) {
+          const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
+          const V2 m = fM[f * NQ2 + t];
+          fQ[2 * (f * NQ2 + t)] = upwind_flux<AR, TC>(m.x, m.y, qP[f], unP[f], sg, sfs[f]);
+        }
+        qlo = static_cast<TC>(sq[t]);
+        qhi = static_cast<TC>(sq[t + NQ2 * (NQ - 1)]);
       }
-      const TC qlo = static_cast<TC>(sq[t]), qhi = static_cast<TC>(sq[t + NQ2 * (NQ - 1)]);
       f5 = upwind_flux<AR, TC>(qlo, wlo, qZ[0], wZ[0], TC(-1), sfs[4]);
       f6 = upwind_flux<AR, TC>(qhi, whi, qZ[1], wZ[1], TC(1), sfs[5]);
     }
@@ -671,10 +729,24 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         }
         // tensorprod_Lift_hexahedral (kern:278-283): face order 1..6; the
         // x/y face fluxes sit at stride 2 (the .x of each (q, un) pair).
-        TC lf = AR::mul(L[0], fQ[2 * (0 * NQ2 + a + NQ * k)]);
-        lf = AR::mad(L[1], fQ[2 * (1 * NQ2 + b + NQ * k)], lf);
-        lf = AR::mad(L[2], fQ[2 * (2 * NQ2 + a + NQ * k)], lf);
-        lf = AR::mad(L[3], fQ[2 * (3 * NQ2 + b + NQ * k)], lf);
+        // Face fluxes: 1, 3 at (i,k) = (a,k), 2, 4 at (j,k) = (b,k).
+        TC fl1, fl2, fl3, fl4;
+        if constexpr (XSPLIT) {
+          const V2 fyk = ypair[a + NQ * k];
+          fl1 = fyk.x;
+          fl3 = fyk.y;
+          fl2 = xq[b + NQ * k];
+          fl4 = xq[FA::XOFF + b + NQ * k];
+        } else {
+          fl1 = fQ[2 * (0 * NQ2 + a + NQ * k)];
+          fl2 = fQ[2 * (1 * NQ2 + b + NQ * k)];
+          fl3 = fQ[2 * (2 * NQ2 + a + NQ * k)];
+          fl4 = fQ[2 * (3 * NQ2 + b + NQ * k)];
+        }
+        TC lf = AR::mul(L[0], fl1);
+        lf = AR::mad(L[1], fl2, lf);
+        lf = AR::mad(L[2], fl3, lf);
+        lf = AR::mad(L[3], fl4, lf);
         lf = AR::mad(L[4], f5, lf);
         lf = AR::mad(L[5], f6, lf);
         // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
