@@ -229,6 +229,32 @@ def stage_bytes_per_dof(mixed):
     return [8 + 24 + 8, 8 + 24 + 8 + 8, 8 + 24 + 8 + 8]
 
 
+def mixed_accuracy(sdg, ops, mesh, fields, dt, nstep):
+    """Error of the mixed form after `nstep` RK3 steps against the FP64 form
+    (fast FP64 GPU path, itself within 1e-12 of the oracle): relative L2,
+    relative max-norm and the relative drift of the FP64 mass diagnostic."""
+    q, u, v, w = fields
+    lgl_w = sdg.lgl_weights(ops.x1D)
+    jac = 1.0 / (8.0 * mesh.Ne)  # (dx dy dz) / 8 on the unit box
+    res = {}
+    for name, flags in (("f64", 0), ("mixed", sdg.FLAG_MIXED)):
+        h = sdg.Handle(ops, mesh, flags)
+        h.set_state(q, u, v, w)
+        mass0, _ = h.diagnostics(lgl_w, jac)
+        h.rk3_steps(dt, nstep)
+        mass, l2 = h.diagnostics(lgl_w, jac)
+        res[name] = (h.get_field(), mass0, mass)
+        h.close()
+    ref, mass0, mass_ref = res["f64"]
+    got, _, mass_got = res["mixed"]
+    d = got - ref
+    return {"nstep": nstep, "against": "FP64 fast GPU path",
+            "rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+            "rel_maxnorm": float(np.abs(d).max() / np.abs(ref).max()),
+            "mass_drift_mixed": float((mass_got - mass0) / abs(mass0)),
+            "mass_drift_f64": float((mass_ref - mass0) / abs(mass0))}
+
+
 def cpu_baseline(workload, seconds):
     """The CPU oracle (restated reference OPT1 path) on all host threads:
     repeated tendency evaluations of the same workload for ~`seconds`."""
@@ -395,6 +421,11 @@ def run_ours(args):
                   "h2d_bytes_per_step": 4 * NA * 8, "d2h_bytes_per_step": NE * 8}
         Hc.close()
 
+    # ---- accuracy of the mixed form against FP64 after nstep steps ----
+    accuracy = None
+    if mixed:
+        accuracy = mixed_accuracy(sdg, ops, mesh, (q, u, v, w), dt, 200)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, args.cpu_seconds)
@@ -423,6 +454,7 @@ def run_ours(args):
                     "h2d_bytes_per_step": NE * 8, "d2h_bytes_per_step": NE * 8,
                     "api": "sdg_set_field + sdg_rk3_steps + sdg_get_field per step"},
             "e2e_cal_tend": e2e_ct,
+            "accuracy": accuracy,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": launches,
