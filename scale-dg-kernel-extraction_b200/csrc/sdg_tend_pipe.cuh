@@ -126,42 +126,49 @@ __device__ __forceinline__ T ld_stream(const T* p) {
 // Placement of node (i,j,k) in the x-line and y-line buffers.  A thread
 // (a,b) touches them in three patterns: its column (a,b,k) for k = 0..Nq-1,
 // its x-line (l,a,b) and its y-line (a,l,b) for l = 0..Nq-1.  Each pattern
-// has a per-thread base and a compile-time step, so the unrolled accesses
-// are one register plus immediates:
-//   column   x: colx(a,b,k&1) + CS*k     y: coly(a,b,k&1) + CS*k
+// has a per-thread part and a compile-time part (k or l unrolled), so the
+// accesses cost a register plus an immediate or one XOR:
+//   column   x: colx(a,b,k)              y: coly(a,b,k)
 //   x-line   xl(xl_base(a,b), l)         y-line  yl(yl_base(a,b), l)
 // Generic orders use the padded layout of tend_kernel (row stride RS,
-// plane stride PS).  For Nq = 8 an XOR swizzle over the 16 eight-byte bank
-// pairs makes every pattern conflict-free (column: i fastest, two j per
-// half-warp; x-line: fixed i, j and two k per half-warp; y-line: fixed j,
-// i and two k):
-//   x(i,j,k) = 16*((j + 8k) >> 1) + ((i ^ j) & 7) + 8*((j + k) & 1)
-//   y(i,j,k) = 16*((i + 8k) >> 1) + ((i ^ j) & 7) + 8*((i + k) & 1)
-// (bijections onto 0..511).  Both line patterns then reduce to
-// x(l,a,b) = y(a,l,b) = (64b + 16(a>>1) + 8((a+b)&1) + a) ^ l, the low three
-// bits of the bracket before "+ a" being zero.  The padded layout costs two
-// wavefronts more per column access.
-template <int NQ>
+// plane stride PS).  At Nq = 8 the layout depends on the word size, because
+// a warp's 32 accesses must fall in distinct banks: 16 eight-byte bank pairs
+// per half-warp for FP64, 32 four-byte banks for FP32.
+//   FP64: an XOR swizzle with x and y buffers of their own,
+//     x(i,j,k) = 16*((j + 8k) >> 1) + ((i ^ j) & 7) + 8*((j + k) & 1)
+//     y(i,j,k) = 16*((i + 8k) >> 1) + ((i ^ j) & 7) + 8*((i + k) & 1)
+//   so that both line patterns reduce to
+//   x(l,a,b) = y(a,l,b) = (64b + 16(a>>1) + 8((a+b)&1) + a) ^ l.
+//   FP32: one layout for both buffers,
+//     f(i,j,k) = 64k + 8(j ^ k) + (i ^ (4(j>>2) + (k&3))),
+//   whose three bit fields are disjoint, so that
+//     column (a,b,k): ((8b + (a ^ 4(b>>2))) ^ (8k + (k&3))) + 64k,
+//     x-line (l,a,b): (64b | 8(a^b) | (4(a>>2) + (b&3))) ^ l,
+//     y-line (a,l,b): (72b + (a ^ (b&3))) ^ (8l + 4(l>>2)).
+//   (The FP64 swizzle, read with four-byte banks, conflicts two ways on
+//   every x-line access; this one is conflict-free on all three patterns.)
+// All are bijections onto 0..511.  The padded layout costs two wavefronts
+// more per column access.
+template <int NQ, int WORD>
 struct LineIdx {
   static constexpr int SIZE = Geo<NQ>::SBUF;
   static constexpr int RS = Geo<NQ>::RS;
-  static constexpr int CS = Geo<NQ>::PS;
-  static __device__ __forceinline__ int colx(int a, int b, int) { return a + RS * b; }
-  static __device__ __forceinline__ int coly(int a, int b, int) { return a + RS * b; }
-  static __device__ __forceinline__ int xl_base(int a, int b) { return RS * a + CS * b; }
+  static constexpr int PS = Geo<NQ>::PS;
+  static __device__ __forceinline__ int colx(int a, int b, int k) { return a + RS * b + PS * k; }
+  static __device__ __forceinline__ int coly(int a, int b, int k) { return a + RS * b + PS * k; }
+  static __device__ __forceinline__ int xl_base(int a, int b) { return RS * a + PS * b; }
   static __device__ __forceinline__ int xl(int base, int l) { return base + l; }
-  static __device__ __forceinline__ int yl_base(int a, int b) { return a + CS * b; }
+  static __device__ __forceinline__ int yl_base(int a, int b) { return a + PS * b; }
   static __device__ __forceinline__ int yl(int base, int l) { return base + RS * l; }
 };
 template <>
-struct LineIdx<8> {
+struct LineIdx<8, 8> {
   static constexpr int SIZE = 512;
-  static constexpr int CS = 64;
-  static __device__ __forceinline__ int colx(int a, int b, int par) {
-    return 16 * (b >> 1) + ((a ^ b) & 7) + 8 * ((b + par) & 1);
+  static __device__ __forceinline__ int colx(int a, int b, int k) {
+    return 16 * (b >> 1) + ((a ^ b) & 7) + 8 * ((b + k) & 1) + 64 * k;
   }
-  static __device__ __forceinline__ int coly(int a, int b, int par) {
-    return 16 * (a >> 1) + ((a ^ b) & 7) + 8 * ((a + par) & 1);
+  static __device__ __forceinline__ int coly(int a, int b, int k) {
+    return 16 * (a >> 1) + ((a ^ b) & 7) + 8 * ((a + k) & 1) + 64 * k;
   }
   static __device__ __forceinline__ int xl_base(int a, int b) {
     return (64 * b + 16 * (a >> 1) + 8 * ((a + b) & 1)) | a;
@@ -169,6 +176,20 @@ struct LineIdx<8> {
   static __device__ __forceinline__ int xl(int base, int l) { return base ^ l; }
   static __device__ __forceinline__ int yl_base(int a, int b) { return xl_base(a, b); }
   static __device__ __forceinline__ int yl(int base, int l) { return base ^ l; }
+};
+template <>
+struct LineIdx<8, 4> {
+  static constexpr int SIZE = 512;
+  static __device__ __forceinline__ int colx(int a, int b, int k) {
+    return ((8 * b + (a ^ (4 * (b >> 2)))) ^ (8 * k + (k & 3))) + 64 * k;
+  }
+  static __device__ __forceinline__ int coly(int a, int b, int k) { return colx(a, b, k); }
+  static __device__ __forceinline__ int xl_base(int a, int b) {
+    return (64 * b) | (8 * (a ^ b)) | (4 * (a >> 2) + (b & 3));
+  }
+  static __device__ __forceinline__ int xl(int base, int l) { return base ^ l; }
+  static __device__ __forceinline__ int yl_base(int a, int b) { return 72 * b + (a ^ (b & 3)); }
+  static __device__ __forceinline__ int yl(int base, int l) { return base ^ (8 * l + 4 * (l >> 2)); }
 };
 
 // Line buffers of the tensor-core contractions (fast FP64, Nq = 8): eight
@@ -231,7 +252,7 @@ struct PipeGeo {
   static constexpr int NP = NQ2 * NQ;
   static constexpr int EPB = NQ2 >= 128 ? 1 : 128 / NQ2;
   static constexpr int THREADS = EPB * NQ2;
-  static constexpr int SBUF = LineIdx<NQ>::SIZE;
+  static constexpr int SBUF = LineIdx<NQ, 8>::SIZE;
 };
 
 // Shared-memory plan of the pipelined kernel.
@@ -364,11 +385,13 @@ __device__ __forceinline__ uint32_t tile_shift(int e0, size_t per_elem) {
 
 // Blocks per SM the kernel is compiled for: what its shared memory allows,
 // but at most 2 for the exact kernels, whose separately rounded arithmetic
-// needs the larger register budget.
+// needs the larger register budget, and for FP64 columns of 9 or more nodes
+// (at the three-block budget of 168 registers they spill 200-300 bytes; two
+// blocks measured 13 % faster at Nq = 10).
 template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE>
 constexpr int pipe_min_blocks() {
   constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE>::MIN_BLOCKS;
-  return (EXACT && m > 2) ? 2 : m;
+  return ((EXACT || (sizeof(TC) == 8 && NQ >= 9)) && m > 2) ? 2 : m;
 }
 
 // The thread bound is the block size rounded up to whole warps (the
@@ -385,7 +408,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
   using AR = Ar<TC, EXACT>;
   using Ctx = TileCtx<TQ, TV, TO, TC>;
   using V2 = typename Pair2<TC>::type;
-  using LI = LineIdx<NQ>;
+  using LI = LineIdx<NQ, static_cast<int>(sizeof(TC))>;
   constexpr int NQ2 = G::NQ2;
   constexpr int NP = G::NP;
   constexpr int EPB = G::EPB;
@@ -576,12 +599,10 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           py[NQ2 * k] = fy[k];
         }
       } else {
-        TC* cx[2] = {sX + LI::colx(a, b, 0), sX + LI::colx(a, b, 1)};
-        TC* cy[2] = {sY + LI::coly(a, b, 0), sY + LI::coly(a, b, 1)};
 #pragma unroll
         for (int k = 0; k < NQ; ++k) {
-          cx[k & 1][LI::CS * k] = fx[k];
-          cy[k & 1][LI::CS * k] = fy[k];
+          sX[LI::colx(a, b, k)] = fx[k];
+          sY[LI::coly(a, b, k)] = fy[k];
         }
       }
     }
@@ -689,20 +710,15 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     if (active) {
       // ---- Phase 4: z-derivative, lift, combine, store ---------------------
       const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
-      // This column's entries of the x/y results: k-plane k, then the
-      // layout's in-plane offset.
-      const TC* cx[2];
-      const TC* cy[2];
-      if constexpr (TENSOR) {
-        cx[0] = cx[1] = sX + TensorIdx8::qx(a, b);
-        cy[0] = cy[1] = sY + TensorIdx8::qy(a, b);
-      } else {
-        cx[0] = sX + LI::colx(a, b, 0);
-        cx[1] = sX + LI::colx(a, b, 1);
-        cy[0] = sY + LI::coly(a, b, 0);
-        cy[1] = sY + LI::coly(a, b, 1);
-      }
-      constexpr int CS = TENSOR ? NQ2 : LI::CS;
+      // This column's entry of the x/y results at node k.
+      auto xres = [&](int k) -> TC {
+        if constexpr (TENSOR) return sX[TensorIdx8::qx(a, b) + NQ2 * k];
+        else return sX[LI::colx(a, b, k)];
+      };
+      auto yres = [&](int k) -> TC {
+        if constexpr (TENSOR) return sY[TensorIdx8::qy(a, b) + NQ2 * k];
+        else return sY[LI::coly(a, b, k)];
+      };
       TC lxy[4];
       if constexpr (!EXACT) {
         lxy[0] = sL[b];
@@ -750,8 +766,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         lf = AR::mad(L[4], f5, lf);
         lf = AR::mad(L[5], f6, lf);
         // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
-        TC acc = AR::mul(e1, cx[k & 1][CS * k]);
-        acc = AR::mad(e2, cy[k & 1][CS * k], acc);
+        TC acc = AR::mul(e1, xres(k));
+        acc = AR::mad(e2, yres(k), acc);
         acc = AR::mad(e3, dz, acc);
         acc = AR::add(acc, lf);
         const TC dqdt = -acc;
