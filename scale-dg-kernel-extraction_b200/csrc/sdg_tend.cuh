@@ -191,6 +191,22 @@ __device__ __forceinline__ void dmma_tile8(double a0, double a1, double b0, doub
   dmma_m8n8k4(*d0, *d1, a1, b1, c0, c1);
 }
 
+// Bulk prefetch of a global range into L2 (TMA engine); addr and bytes are
+// multiples of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes)
+               : "memory");
+}
+
+// Prefetch of bytes [lo, hi) of an array into L2, shrunk to whole 16-byte
+// words inside the range (so it never touches a byte outside it).
+__device__ __forceinline__ void prefetch_l2_range(const void* base, size_t lo, size_t hi) {
+  const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+  const uintptr_t a0 = (b + lo + 15) & ~uintptr_t(15);
+  const uintptr_t a1 = (b + hi) & ~uintptr_t(15);
+  if (a1 > a0) bulk_prefetch_l2(reinterpret_cast<const void*>(a0), static_cast<uint32_t>(a1 - a0));
+}
+
 __device__ __forceinline__ double absv(double x) { return fabs(x); }
 __device__ __forceinline__ float absv(float x) { return fabsf(x); }
 
@@ -236,6 +252,9 @@ struct TendArgs {
   int nelem;            // elements in this launch
   double rk_a, rk_b, dt;
   int* status;          // device status word: nonzero after a timed-out wait
+  // One-tile-per-block kernel: block b prefetches into L2 the inputs of
+  // block b + prefetch_dist (about one resident wave ahead); 0 disables.
+  int prefetch_dist;
   // Batched launches (pipelined kernel only): per-instance arrays and a
   // table of element tiles.  Null for a single instance, whose tiles are
   // the consecutive elements elem0 .. elem0+nelem-1 of the arrays above.
@@ -304,6 +323,23 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
   TC qc[NQ];                   // column of q
   TC fz[NQ];                   // column of q*w
   TC wlo = TC(0), whi = TC(0);
+
+  // Blocks run in launch order, so the block one resident wave later starts
+  // about when this one ends: bring its inputs into L2 now.
+  if (A.prefetch_dist > 0 && threadIdx.x == 0) {
+    const long nb = (static_cast<long>(A.nelem) + G::EPB - 1) / G::EPB;
+    const long pblk = static_cast<long>(blockIdx.x) + A.prefetch_dist;
+    if (pblk < nb) {
+      const long e0 = A.elem0 + pblk * G::EPB;
+      const long e1 = A.elem0 + min(static_cast<long>(A.nelem), (pblk + 1) * G::EPB);
+      prefetch_l2_range(A.q, e0 * G::NP * sizeof(TQ), e1 * G::NP * sizeof(TQ));
+      prefetch_l2_range(A.u, e0 * G::NP * sizeof(TV), e1 * G::NP * sizeof(TV));
+      prefetch_l2_range(A.v, e0 * G::NP * sizeof(TV), e1 * G::NP * sizeof(TV));
+      prefetch_l2_range(A.w, e0 * G::NP * sizeof(TV), e1 * G::NP * sizeof(TV));
+      if (STAGE && A.rk_a != 0.0)
+        prefetch_l2_range(A.q0, e0 * G::NP * sizeof(double), e1 * G::NP * sizeof(double));
+    }
+  }
 
   // ---- Phase 1: load the column, form the volume fluxes ------------------
   if (active) {
@@ -418,12 +454,13 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
   if (!active) return;
 
   // ---- Phase 4: z-derivative, lift and combine in the column thread -------
-  TC dz[NQ];
-#pragma unroll
-  for (int k = 0; k < NQ; ++k)
-    dz[k] = contract<NQ, ORDER, AR, TC>(
+  // The z-derivative of node k is formed where it is used, so no column of
+  // results is held in registers (it matters for the long columns of p > 10).
+  auto dz = [&](int k) {
+    return contract<NQ, ORDER, AR, TC>(
         [&](int l) { return fz[l]; },                 // vec_in_z(i,j,l)
         [&](int l) { return D.d[k * NQ + l]; });      // Mat_tr(l,k)
+  };
 
   const TC* es = A.escale + 3 * static_cast<long>(e);
   const TC e1 = es[0], e2 = es[1], e3 = es[2];
@@ -441,7 +478,7 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
     // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
     TC acc = AR::mul(e1, sX[a + RS * b + PS * k]);
     acc = AR::mad(e2, sY[a + RS * b + PS * k], acc);
-    acc = AR::mad(e3, dz[k], acc);
+    acc = AR::mad(e3, dz(k), acc);
     acc = AR::add(acc, lf);
     const TC dqdt = -acc;
     const long n = base + t + NQ2 * k;

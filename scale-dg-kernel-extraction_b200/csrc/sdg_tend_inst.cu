@@ -66,6 +66,7 @@ int run(const LaunchSpec& s) {
   a.rk_b = s.rk_b;
   a.dt = s.dt;
   a.status = s.status;
+  a.prefetch_dist = 0;
   a.insts = static_cast<const BatchInst*>(s.batch_insts);
   a.tiles = static_cast<const BatchTile*>(s.batch_tiles);
   a.ntiles = s.batch_ntiles;
@@ -107,20 +108,33 @@ int run(const LaunchSpec& s) {
         carve_done = true;
       }
       if (s.nelem <= 0) return 0;
+      a.prefetch_dist = 8 * (s.num_sms > 0 ? s.num_sms : 148);
       const int blocks = (s.nelem + G::EPB - 1) / G::EPB;
       kern<<<blocks, G::THREADS, smem, s.stream>>>(a, d);
       return static_cast<int>(cudaGetLastError());
     }
   }
-  auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE>;
-  static bool attr_done = false;  // per instantiation
-  if (smem > 48 * 1024 && !attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(
-        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  // The fast FP64 kernels with columns of 12 or more nodes are built for two
+  // resident blocks: left free they take 160-254 registers, one block of
+  // 144-256 threads per SM; capped they spill but measured 1.1-1.6x faster
+  // (p = 11: 29.5 -> 48.5 G DOF-updates/s, p = 15: 47.5 -> 53.0).
+  constexpr int MB = (!EXACT && NQ >= 12) ? 2 : 1;
+  auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, MB>;
+  static int resident = 0;  // blocks per SM, per instantiation
+  if (resident == 0) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(
+          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e != cudaSuccess) return static_cast<int>(e);
+    }
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    int nb = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::THREADS, smem);
     if (e != cudaSuccess) return static_cast<int>(e);
-    attr_done = true;
+    resident = nb > 0 ? nb : 1;
   }
   if (s.nelem <= 0) return 0;
+  a.prefetch_dist = resident * (s.num_sms > 0 ? s.num_sms : 148);
   const int blocks = (s.nelem + G::EPB - 1) / G::EPB;
   kern<<<blocks, G::THREADS, smem, s.stream>>>(a, d);
   return static_cast<int>(cudaGetLastError());

@@ -104,13 +104,6 @@ __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bulk prefetch of a global range into L2 (TMA engine); addr and bytes are
-// multiples of 16.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes)
-               : "memory");
-}
-
 // Orders this thread's shared-memory writes before later bulk copies (async
 // proxy) into the same bytes.
 __device__ __forceinline__ void fence_proxy_async_smem() {
@@ -391,7 +384,7 @@ __device__ __forceinline__ uint32_t tile_shift(int e0, size_t per_elem) {
 template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE>
 constexpr int pipe_min_blocks() {
   constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE>::MIN_BLOCKS;
-  return ((EXACT || (sizeof(TC) == 8 && NQ >= 9)) && m > 2) ? 2 : m;
+  return ((EXACT || (sizeof(TC) == 8 && NQ >= 9) || NQ >= 12) && m > 2) ? 2 : m;
 }
 
 // The thread bound is the block size rounded up to whole warps (the
