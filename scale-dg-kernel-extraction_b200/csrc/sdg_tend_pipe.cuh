@@ -582,6 +582,9 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
       }
     }
     __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
+    // Plus-side face values of the x/y faces (face node t).
+    TC qP[4], unP[4];
+    unsigned in_tile = 0;  // bit f: face f's neighbour is an element of this tile
     if (active) {
       if constexpr (TENSOR) {
         TC* px = sX + TensorIdx8::px(a, b);
@@ -598,15 +601,48 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           sY[LI::coly(a, b, k)] = fy[k];
         }
       }
+      // A neighbour in this tile stored its minus-side values of the shared
+      // face (the face opposite f: -y/+y and +x/-x swap) in its face area
+      // before the barrier above; phase 2 replaces them with fluxes only
+      // after the next barrier.  Read them here rather than gathering them
+      // from global memory.  The values are the same, so are the results.
+      if constexpr (EPB > 1) {
+        TC* const fa0 = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          const int d = pbc[f] - C.e0 * NP;
+          if (pbc[f] >= 0 && d >= 0 && d < C.n * NP) {
+            in_tile |= 1u << f;
+            const TC* nfa = fa0 + (d / NP) * FA::ELEM;
+            if constexpr (XSPLIT) {
+              if (f == 1 || f == 3) {
+                const int xi = (f == 1 ? FA::XOFF : 0) + t;
+                qP[f] = nfa[xi];
+                unP[f] = nfa[FA::XA + xi];
+              } else {
+                const V2 m = reinterpret_cast<const V2*>(nfa + FA::Y0)[(f == 0 ? NQ2 : 0) + t];
+                qP[f] = m.x;
+                unP[f] = m.y;
+              }
+            } else {
+              const V2 m = reinterpret_cast<const V2*>(nfa)[((f + 2) & 3) * NQ2 + t];
+              qP[f] = m.x;
+              unP[f] = m.y;
+            }
+          }
+        }
+      }
     }
     __syncthreads();
 
     // ---- Loads whose latency phase 3 covers --------------------------------
-    // Plus-side face values of the x/y faces (face node t) and z faces.
-    TC qP[4], unP[4], qZ[2], wZ[2];
+    // The other plus-side face values: x/y faces whose neighbour lies
+    // outside the tile (or in the caller's halo), and the z faces.
+    TC qZ[2], wZ[2];
     if (active) {
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
+        if (in_tile & (1u << f)) continue;
         const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
                                        : static_cast<long>(-1 - pbc[f]) + t;
         qP[f] = static_cast<TC>(ldro(C.q + idx));
