@@ -543,6 +543,47 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     TC* sX = reinterpret_cast<TC*>(sb + P::OFF_U) + s * G::SBUF;
     TC* sY = reinterpret_cast<TC*>(sb + P::OFF_V) + s * G::SBUF;
 
+    // ---- Plus-side face values ---------------------------------------------
+    // x/y faces whose neighbour lies outside the tile (or in the caller's
+    // halo) and the z faces come from global memory; a neighbour inside the
+    // tile is read from shared memory after phase 1.  The global loads are
+    // issued before phase 1, so that phase 1 and the line contractions cover
+    // their latency, except in the FP32 kernels with one element per tile,
+    // which measured faster (-4 % register pressure in phase 1) with the
+    // loads after the line buffers are published.
+    TC qP[4], unP[4], qZ[2], wZ[2];
+    unsigned in_tile = 0;  // bit f: face f's neighbour is an element of this tile
+    if constexpr (EPB > 1) {
+      if (active) {
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          const int d = pbc[f] - C.e0 * NP;
+          if (pbc[f] >= 0 && d >= 0 && d < C.n * NP) in_tile |= 1u << f;
+        }
+      }
+    }
+    auto gather = [&]() {
+      if (!active) return;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        if (in_tile & (1u << f)) continue;
+        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
+                                       : static_cast<long>(-1 - pbc[f]) + t;
+        qP[f] = static_cast<TC>(ldro(C.q + idx));
+        unP[f] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx) : ldro(C.v + idx));
+      }
+#pragma unroll
+      for (int z = 0; z < 2; ++z) {
+        const int f = 4 + z;
+        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
+                                       : static_cast<long>(-1 - pbc[f]) + t;
+        qZ[z] = static_cast<TC>(ldro(C.q + idx));
+        wZ[z] = static_cast<TC>(ldro(C.w + idx));
+      }
+    };
+    constexpr bool EARLY = EPB > 1 || sizeof(TC) == 8;
+    if constexpr (EARLY) gather();
+
     // ---- Phase 1: the column's volume fluxes and minus-side face values ---
     // q*w replaces w in place: each thread reads and writes only its own
     // column there, so the z-flux column waits in shared memory for phase 4.
@@ -582,9 +623,6 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
       }
     }
     __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
-    // Plus-side face values of the x/y faces (face node t).
-    TC qP[4], unP[4];
-    unsigned in_tile = 0;  // bit f: face f's neighbour is an element of this tile
     if (active) {
       if constexpr (TENSOR) {
         TC* px = sX + TensorIdx8::px(a, b);
@@ -610,9 +648,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         TC* const fa0 = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-          const int d = pbc[f] - C.e0 * NP;
-          if (pbc[f] >= 0 && d >= 0 && d < C.n * NP) {
-            in_tile |= 1u << f;
+          if (in_tile & (1u << f)) {
+            const int d = pbc[f] - C.e0 * NP;
             const TC* nfa = fa0 + (d / NP) * FA::ELEM;
             if constexpr (XSPLIT) {
               if (f == 1 || f == 3) {
@@ -634,29 +671,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
       }
     }
     __syncthreads();
+    if constexpr (!EARLY) gather();
 
-    // ---- Loads whose latency phase 3 covers --------------------------------
-    // The other plus-side face values: x/y faces whose neighbour lies
-    // outside the tile (or in the caller's halo), and the z faces.
-    TC qZ[2], wZ[2];
-    if (active) {
-#pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        if (in_tile & (1u << f)) continue;
-        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
-                                       : static_cast<long>(-1 - pbc[f]) + t;
-        qP[f] = static_cast<TC>(ldro(C.q + idx));
-        unP[f] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx) : ldro(C.v + idx));
-      }
-#pragma unroll
-      for (int z = 0; z < 2; ++z) {
-        const int f = 4 + z;
-        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
-                                       : static_cast<long>(-1 - pbc[f]) + t;
-        qZ[z] = static_cast<TC>(ldro(C.q + idx));
-        wZ[z] = static_cast<TC>(ldro(C.w + idx));
-      }
-    }
     constexpr int NQ0 = STAGE ? NQ : 1;
     double q0r[NQ0];
     const bool use_q0 = STAGE && A.rk_a != 0.0;
