@@ -151,6 +151,47 @@ __device__ __forceinline__ T contract(FA A, FB B) {
   }
 }
 
+// Orders (NQ = p + 1) whose fast FP32 kernels advance the x and y lines of a
+// thread together with packed FMAs (contract2).  Measured per order on the
+// pipelined kernel (G DOF-updates/s, paired vs scalar): p = 3 104.2 / 102.5,
+// p = 7 146.7 / 140.7, p = 10 128.5 / 121.2, p = 11 111.4 / 102.3, p = 12
+// 119.9 / 99.4; slower at p = 4, 5, 8 (101.5 / 106.0, 106.7 / 114.1,
+// 109.1 / 118.7), where the wider live range costs a resident block.
+template <int NQ>
+constexpr bool kPairedLinesPipe = NQ == 4 || NQ == 8 || NQ >= 11;
+// The one-tile-per-block kernel, which the fast FP32 forms run at p >= 13:
+// p = 13 78.2 / 63.5, p = 14 81.9 / 78.1, p = 15 92.7 / 86.9.
+template <int NQ>
+constexpr bool kPairedLinesBlock = NQ >= 14;
+
+// Two fast FP32 contractions with one coefficient row: component c of the
+// result is contract<NQ, ORDER, Ar<float, false>, float>(A, B_c), step for
+// step.  The packed sm_100 instructions (__ffma2_rn, __fmul2_rn, __fadd2_rn)
+// round each component exactly as the scalar fmaf/__fmul_rn/__fadd_rn, so
+// the results are the scalar contraction's bits at half the instructions.
+template <int NQ, int ORDER, typename FA>
+__device__ __forceinline__ float2 contract2(FA A, const float2 (&B)[NQ]) {
+  auto dup = [](float x) { return make_float2(x, x); };
+  if constexpr (NQ <= 8 || ORDER == kOrderGeneral) {
+    float2 t = __fmul2_rn(dup(A(0)), B[0]);
+#pragma unroll
+    for (int l = 1; l < NQ; ++l) t = __ffma2_rn(dup(A(l)), B[l], t);
+    return t;
+  } else {
+    constexpr int N3 = Geo<NQ>::N3;
+    float2 t1 = __fmul2_rn(dup(A(0)), B[0]);
+#pragma unroll
+    for (int l = 1; l < N3; ++l) t1 = __ffma2_rn(dup(A(l)), B[l], t1);
+    float2 t2 = __fmul2_rn(dup(A(N3)), B[N3]);
+#pragma unroll
+    for (int l = N3 + 1; l < 2 * N3; ++l) t2 = __ffma2_rn(dup(A(l)), B[l], t2);
+    float2 t3 = __fmul2_rn(dup(A(2 * N3)), B[2 * N3]);
+#pragma unroll
+    for (int l = 2 * N3 + 1; l < NQ; ++l) t3 = __ffma2_rn(dup(A(l)), B[l], t3);
+    return __fadd2_rn(__fadd2_rn(t1, t2), t3);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // FP64 tensor-core line contractions (fast FP64 kernels, Nq = 8)
 // ---------------------------------------------------------------------------
@@ -430,6 +471,18 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
                    &d1);
         sY[2 * qd + RS * g + PS * T] = d0;
         sY[2 * qd + 1 + RS * g + PS * T] = d1;
+      }
+    } else if constexpr (sizeof(TC) == 4 && !EXACT && kPairedLinesBlock<NQ>) {
+      // x line (a,b) and y line (a,b) share the coefficient row D(i, .).
+      float2 ln[NQ];
+#pragma unroll
+      for (int l = 0; l < NQ; ++l)
+        ln[l] = make_float2(sX[l + RS * a + PS * b], sY[a + RS * l + PS * b]);
+#pragma unroll
+      for (int i = 0; i < NQ; ++i) {
+        const float2 r = contract2<NQ, ORDER>([&](int l) { return D.d[i * NQ + l]; }, ln);
+        sX[i + RS * a + PS * b] = r.x;
+        sY[a + RS * i + PS * b] = r.y;
       }
     } else {
       TC line[NQ];

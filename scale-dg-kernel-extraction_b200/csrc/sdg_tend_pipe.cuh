@@ -698,20 +698,34 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           *reinterpret_cast<double2*>(py + TI::qy(2 * qd, g)) = make_double2(d0, d1);
         }
       } else {
-        TC line[NQ];
         const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
+        if constexpr (sizeof(TC) == 4 && !EXACT && kPairedLinesPipe<NQ>) {
+          // Fast FP32: the x line (a,b) and the y line (a,b) take the same
+          // coefficient row D(i, .), so one packed FMA advances both.
+          float2 ln[NQ];
 #pragma unroll
-        for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
+          for (int l = 0; l < NQ; ++l) ln[l] = make_float2(sX[LI::xl(lbx, l)], sY[LI::yl(lby, l)]);
 #pragma unroll
-        for (int i = 0; i < NQ; ++i)
-          sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
-              [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+          for (int i = 0; i < NQ; ++i) {
+            const float2 r = contract2<NQ, ORDER>([&](int l) { return D.d[i * NQ + l]; }, ln);
+            sX[LI::xl(lbx, i)] = r.x;
+            sY[LI::yl(lby, i)] = r.y;
+          }
+        } else {
+          TC line[NQ];
 #pragma unroll
-        for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
+          for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
 #pragma unroll
-        for (int j = 0; j < NQ; ++j)
-          sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, TC>(
-              [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+          for (int i = 0; i < NQ; ++i)
+            sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
+                [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+#pragma unroll
+          for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
+#pragma unroll
+          for (int j = 0; j < NQ; ++j)
+            sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, TC>(
+                [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+        }
       }
       // The line buffers live in the slot that the next refill overwrites.
       fence_proxy_async_smem();
