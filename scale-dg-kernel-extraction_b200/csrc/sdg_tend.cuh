@@ -164,30 +164,31 @@ constexpr bool kPairedLinesPipe = NQ == 4 || NQ == 8 || NQ >= 11;
 template <int NQ>
 constexpr bool kPairedLinesBlock = NQ >= 14;
 
-// Two fast FP32 contractions with one coefficient row: component c of the
-// result is contract<NQ, ORDER, Ar<float, false>, float>(A, B_c), step for
-// step.  The packed sm_100 instructions (__ffma2_rn, __fmul2_rn, __fadd2_rn)
-// round each component exactly as the scalar fmaf/__fmul_rn/__fadd_rn, so
-// the results are the scalar contraction's bits at half the instructions.
-template <int NQ, int ORDER, typename FA>
-__device__ __forceinline__ float2 contract2(FA A, const float2 (&B)[NQ]) {
+// Two fast FP32 contractions in one: component c of the result is
+// contract<NQ, ORDER, Ar<float, false>, float>(A, B_c), step for step, where
+// A(l) is shared and B(l) holds both second factors.  The packed sm_100
+// instructions (__ffma2_rn, __fmul2_rn, __fadd2_rn) round each component
+// exactly as the scalar fmaf/__fmul_rn/__fadd_rn, so the results are the
+// scalar contraction's bits at half the instructions.
+template <int NQ, int ORDER, typename FA, typename FB>
+__device__ __forceinline__ float2 contract2(FA A, FB B) {
   auto dup = [](float x) { return make_float2(x, x); };
   if constexpr (NQ <= 8 || ORDER == kOrderGeneral) {
-    float2 t = __fmul2_rn(dup(A(0)), B[0]);
+    float2 t = __fmul2_rn(dup(A(0)), B(0));
 #pragma unroll
-    for (int l = 1; l < NQ; ++l) t = __ffma2_rn(dup(A(l)), B[l], t);
+    for (int l = 1; l < NQ; ++l) t = __ffma2_rn(dup(A(l)), B(l), t);
     return t;
   } else {
     constexpr int N3 = Geo<NQ>::N3;
-    float2 t1 = __fmul2_rn(dup(A(0)), B[0]);
+    float2 t1 = __fmul2_rn(dup(A(0)), B(0));
 #pragma unroll
-    for (int l = 1; l < N3; ++l) t1 = __ffma2_rn(dup(A(l)), B[l], t1);
-    float2 t2 = __fmul2_rn(dup(A(N3)), B[N3]);
+    for (int l = 1; l < N3; ++l) t1 = __ffma2_rn(dup(A(l)), B(l), t1);
+    float2 t2 = __fmul2_rn(dup(A(N3)), B(N3));
 #pragma unroll
-    for (int l = N3 + 1; l < 2 * N3; ++l) t2 = __ffma2_rn(dup(A(l)), B[l], t2);
-    float2 t3 = __fmul2_rn(dup(A(2 * N3)), B[2 * N3]);
+    for (int l = N3 + 1; l < 2 * N3; ++l) t2 = __ffma2_rn(dup(A(l)), B(l), t2);
+    float2 t3 = __fmul2_rn(dup(A(2 * N3)), B(2 * N3));
 #pragma unroll
-    for (int l = 2 * N3 + 1; l < NQ; ++l) t3 = __ffma2_rn(dup(A(l)), B[l], t3);
+    for (int l = 2 * N3 + 1; l < NQ; ++l) t3 = __ffma2_rn(dup(A(l)), B(l), t3);
     return __fadd2_rn(__fadd2_rn(t1, t2), t3);
   }
 }
@@ -480,7 +481,8 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
         ln[l] = make_float2(sX[l + RS * a + PS * b], sY[a + RS * l + PS * b]);
 #pragma unroll
       for (int i = 0; i < NQ; ++i) {
-        const float2 r = contract2<NQ, ORDER>([&](int l) { return D.d[i * NQ + l]; }, ln);
+        const float2 r = contract2<NQ, ORDER>([&](int l) { return D.d[i * NQ + l]; },
+                                              [&](int l) { return ln[l]; });
         sX[i + RS * a + PS * b] = r.x;
         sY[a + RS * i + PS * b] = r.y;
       }

@@ -707,7 +707,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           for (int l = 0; l < NQ; ++l) ln[l] = make_float2(sX[LI::xl(lbx, l)], sY[LI::yl(lby, l)]);
 #pragma unroll
           for (int i = 0; i < NQ; ++i) {
-            const float2 r = contract2<NQ, ORDER>([&](int l) { return D.d[i * NQ + l]; }, ln);
+            const float2 r = contract2<NQ, ORDER>([&](int l) { return D.d[i * NQ + l]; },
+                                                  [&](int l) { return ln[l]; });
             sX[LI::xl(lbx, i)] = r.x;
             sY[LI::yl(lby, i)] = r.y;
           }
