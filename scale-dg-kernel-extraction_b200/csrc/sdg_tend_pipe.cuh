@@ -378,12 +378,16 @@ __device__ __forceinline__ uint32_t tile_shift(int e0, size_t per_elem) {
 
 // Blocks per SM the kernel is compiled for: what its shared memory allows,
 // but at most 2 for the exact kernels, whose separately rounded arithmetic
-// needs the larger register budget, and for FP64 columns of 9 or more nodes
-// (at the three-block budget of 168 registers they spill 200-300 bytes; two
-// blocks measured 13 % faster at Nq = 10).
+// needs the larger register budget, for FP64 columns of 9 or more nodes (at
+// the three-block budget of 168 registers they spill 200-300 bytes; two
+// blocks measured 13 % faster at Nq = 10, and four spilling blocks 8 % slower
+// at Nq = 9) and for all columns of 12 or more nodes; and at most 3 for the
+// fast FP64 kernels at Nq = 7 (at the four-block budget of 128 registers they
+// spill 36 bytes; three blocks measured 10 % faster: 62.7 -> 69.1 G).
 template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE>
 constexpr int pipe_min_blocks() {
   constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE>::MIN_BLOCKS;
+  if constexpr (sizeof(TC) == 8 && !EXACT && NQ == 7) return m > 3 ? 3 : m;
   return ((EXACT || (sizeof(TC) == 8 && NQ >= 9) || NQ >= 12) && m > 2) ? 2 : m;
 }
 
