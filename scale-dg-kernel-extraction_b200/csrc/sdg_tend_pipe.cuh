@@ -142,6 +142,16 @@ __device__ __forceinline__ T ld_stream(const T* p) {
 //   every x-line access; this one is conflict-free on all three patterns.)
 // All are bijections onto 0..511.  The padded layout costs two wavefronts
 // more per column access.
+//   Nq = 4, FP64: f(i,j,k) = 16k + 4(j ^ k) + (i ^ k), so that
+//     column (a,b,k): 16k + (t ^ 5k) with t = a + 4b,
+//     x-line (l,a,b): (16b + 4(a^b) + b) ^ l,
+//     y-line (a,l,b): (20b + (a^b)) ^ 4l,
+//   each 16 distinct eight-byte bank pairs over an element (a half-warp);
+//   the padded layout conflicts two ways on column accesses there (FP64
+//   p = 3: 78.2 -> 80.7 G with this one).  The same map is conflict-free for
+//   FP32 as well (elements 80 words apart, 16 mod 32), but its XOR
+//   addressing took the FP32 kernels from 96 to 111 registers and one
+//   resident block fewer: 101.5 against 104.0 G, so FP32 keeps the padding.
 template <int NQ, int WORD>
 struct LineIdx {
   static constexpr int SIZE = Geo<NQ>::SBUF;
@@ -169,6 +179,49 @@ struct LineIdx<8, 8> {
   static __device__ __forceinline__ int xl(int base, int l) { return base ^ l; }
   static __device__ __forceinline__ int yl_base(int a, int b) { return xl_base(a, b); }
   static __device__ __forceinline__ int yl(int base, int l) { return base ^ l; }
+};
+// Skewed linear layouts (FP64, Nq = 6, 7): x(i,j,k) = QX*i_x + ..., a
+// permutation of (i, j, k) weighted (Q, 1, Nq) per buffer, elements SIZE
+// words apart.  Every pattern is a register plus an immediate.
+template <int NQ, int X0, int X1, int X2, int QX, int Y0, int Y1, int Y2, int QY, int E>
+struct SkewIdx {
+  static constexpr int SIZE = E;
+  template <int P0, int P1, int P2, int Q>
+  static __device__ __forceinline__ int w(int i, int j, int k) {
+    const int idx[3] = {i, j, k};
+    return Q * idx[P0] + idx[P1] + NQ * idx[P2];
+  }
+  // Weight of i in the x layout and of j in the y layout (the line index).
+  static constexpr int WXI = X0 == 0 ? QX : (X1 == 0 ? 1 : NQ);
+  static constexpr int WYJ = Y0 == 1 ? QY : (Y1 == 1 ? 1 : NQ);
+  static __device__ __forceinline__ int colx(int a, int b, int k) { return w<X0, X1, X2, QX>(a, b, k); }
+  static __device__ __forceinline__ int coly(int a, int b, int k) { return w<Y0, Y1, Y2, QY>(a, b, k); }
+  static __device__ __forceinline__ int xl_base(int a, int b) { return w<X0, X1, X2, QX>(0, a, b); }
+  static __device__ __forceinline__ int xl(int base, int l) { return base + WXI * l; }
+  static __device__ __forceinline__ int yl_base(int a, int b) { return w<Y0, Y1, Y2, QY>(a, 0, b); }
+  static __device__ __forceinline__ int yl(int base, int l) { return base + WYJ * l; }
+};
+//   Nq = 6: x = 38i + j + 6k, y = 38j + i + 6k, 228 words per element;
+//   Nq = 7: x = 49i + k + 7j, y = 49j + k + 7i, 343 words per element.
+// Found by exhaustive search over permutations, Q and the element stride
+// against the warp layout of the 108- and 98-thread blocks: line-buffer
+// wavefronts per tile 276 -> 204 (Nq = 6, ideal 168) and 294 -> 203
+// (Nq = 7, ideal 196) against the padded layout.
+template <>
+struct LineIdx<6, 8> : SkewIdx<6, 0, 1, 2, 38, 1, 0, 2, 38, 228> {};
+template <>
+struct LineIdx<7, 8> : SkewIdx<7, 0, 2, 1, 49, 1, 2, 0, 49, 343> {};
+template <>
+struct LineIdx<4, 8> {
+  static constexpr int SIZE = 80;
+  static __device__ __forceinline__ int colx(int a, int b, int k) {
+    return 16 * k + ((a + 4 * b) ^ (5 * k));
+  }
+  static __device__ __forceinline__ int coly(int a, int b, int k) { return colx(a, b, k); }
+  static __device__ __forceinline__ int xl_base(int a, int b) { return 16 * b + 4 * (a ^ b) + b; }
+  static __device__ __forceinline__ int xl(int base, int l) { return base ^ l; }
+  static __device__ __forceinline__ int yl_base(int a, int b) { return 20 * b + (a ^ b); }
+  static __device__ __forceinline__ int yl(int base, int l) { return base ^ (4 * l); }
 };
 template <>
 struct LineIdx<8, 4> {
@@ -245,7 +298,6 @@ struct PipeGeo {
   static constexpr int NP = NQ2 * NQ;
   static constexpr int EPB = NQ2 >= 128 ? 1 : 128 / NQ2;
   static constexpr int THREADS = EPB * NQ2;
-  static constexpr int SBUF = LineIdx<NQ, 8>::SIZE;
 };
 
 // Shared-memory plan of the pipelined kernel.
@@ -263,7 +315,8 @@ struct PipePlan {
   // x- and y-line buffers once the tile's columns are in registers.
   static constexpr size_t QB = r16(sizeof(TQ) * EPB * NP + 32);
   static constexpr size_t VB =
-      mx(r16(sizeof(TV) * EPB * NP + 32), r16(sizeof(TC) * EPB * G::SBUF));
+      mx(r16(sizeof(TV) * EPB * NP + 32),
+         r16(sizeof(TC) * EPB * LineIdx<NQ, static_cast<int>(sizeof(TC))>::SIZE));
   static constexpr size_t EB = r16(sizeof(TC) * 3 * EPB + 32);  // escale rows
   static constexpr size_t FB = r16(sizeof(TC) * 6 * EPB + 32);  // fscale rows
   static constexpr size_t OFF_U = QB;
@@ -544,8 +597,8 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     static_assert(sizeof(TV) == sizeof(TC), "w and q*w share their slots");
     TC* sz = reinterpret_cast<TC*>(sb + P::OFF_W + shv) + s * NP;
     // Line buffers in the u and v regions (valid after the column reads).
-    TC* sX = reinterpret_cast<TC*>(sb + P::OFF_U) + s * G::SBUF;
-    TC* sY = reinterpret_cast<TC*>(sb + P::OFF_V) + s * G::SBUF;
+    TC* sX = reinterpret_cast<TC*>(sb + P::OFF_U) + s * LI::SIZE;
+    TC* sY = reinterpret_cast<TC*>(sb + P::OFF_V) + s * LI::SIZE;
 
     // ---- Plus-side face values ---------------------------------------------
     // x/y faces whose neighbour lies outside the tile (or in the caller's
