@@ -202,15 +202,27 @@ struct SkewIdx {
   static __device__ __forceinline__ int yl(int base, int l) { return base + WYJ * l; }
 };
 //   Nq = 6: x = 38i + j + 6k, y = 38j + i + 6k, 228 words per element;
-//   Nq = 7: x = 49i + k + 7j, y = 49j + k + 7i, 343 words per element.
+//   Nq = 7: x = 49i + k + 7j, y = 49j + k + 7i, 343 words per element;
+//   Nq = 9: x = 89i + j + 9k, y = 89j + i + 9k;
+//   Nq = 10: x = 102i + j + 10k, y = 106j + i + 10k.
 // Found by exhaustive search over permutations, Q and the element stride
-// against the warp layout of the 108- and 98-thread blocks: line-buffer
-// wavefronts per tile 276 -> 204 (Nq = 6, ideal 168) and 294 -> 203
-// (Nq = 7, ideal 196) against the padded layout.
+// against the warp layout of each block (one element per tile from Nq = 9
+// on), with the shared-memory plan kept at its resident-block count.  Line-
+// buffer wavefronts per tile against the padded layout (ideal): Nq = 6
+// 276 -> 204 (168), Nq = 7 294 -> 203 (196), Nq = 9 261 -> 216 (216),
+// Nq = 10 460 -> 330 (280); measured FP64 p = 5 +5 %, p = 6 +11 %, p = 8
+// +7 %, p = 9 +10 %.  Layouts that reached their ideal but measured no gain
+// were left out: FP64 Nq = 11 (429 -> 352; 66.6 against 67.6 G) and FP32
+// Nq = 10 (250 -> 190; 109.2 against 112.9 G).
 template <>
 struct LineIdx<6, 8> : SkewIdx<6, 0, 1, 2, 38, 1, 0, 2, 38, 228> {};
 template <>
 struct LineIdx<7, 8> : SkewIdx<7, 0, 2, 1, 49, 1, 2, 0, 49, 343> {};
+template <>
+struct LineIdx<9, 8> : SkewIdx<9, 0, 1, 2, 89, 1, 0, 2, 89, 794> {};
+template <>
+struct LineIdx<10, 8> : SkewIdx<10, 0, 1, 2, 102, 1, 0, 2, 106, 1054> {};
+
 template <>
 struct LineIdx<4, 8> {
   static constexpr int SIZE = 80;
