@@ -211,13 +211,20 @@ struct SkewIdx {
 // buffer wavefronts per tile against the padded layout (ideal): Nq = 6
 // 276 -> 204 (168), Nq = 7 294 -> 203 (196), Nq = 9 261 -> 216 (216),
 // Nq = 10 460 -> 330 (280); measured FP64 p = 5 +5 %, p = 6 +11 %, p = 8
-// +7 %, p = 9 +10 %.  Layouts that reached their ideal but measured no gain
+// +7 %, p = 9 +10 %.  FP32 (four-byte banks, 32-lane groups): Nq = 6
+// x = 36i + j + 6k, y = 38j + i + 6k (150 -> 114, ideal 96) and Nq = 7
+// x = 49k + i + 7j, y = 49j + k + 7i (168 -> 140, ideal 112); measured mixed
+// p = 5 +2 %, p = 6 +2 %.  Layouts that reached their ideal but measured no gain
 // were left out: FP64 Nq = 11 (429 -> 352; 66.6 against 67.6 G) and FP32
 // Nq = 10 (250 -> 190; 109.2 against 112.9 G).
 template <>
 struct LineIdx<6, 8> : SkewIdx<6, 0, 1, 2, 38, 1, 0, 2, 38, 228> {};
 template <>
 struct LineIdx<7, 8> : SkewIdx<7, 0, 2, 1, 49, 1, 2, 0, 49, 343> {};
+template <>
+struct LineIdx<6, 4> : SkewIdx<6, 0, 1, 2, 36, 1, 0, 2, 38, 228> {};
+template <>
+struct LineIdx<7, 4> : SkewIdx<7, 2, 0, 1, 49, 1, 2, 0, 49, 343> {};
 template <>
 struct LineIdx<9, 8> : SkewIdx<9, 0, 1, 2, 89, 1, 0, 2, 89, 794> {};
 template <>
