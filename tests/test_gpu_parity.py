@@ -212,10 +212,14 @@ def test_kernel_variants_bitwise(p, variant):
 
 
 @pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE])
-def test_mixed_variants_agree(variant):
-    p, dims, nstep = 7, (4, 3, 5), 10
+@pytest.mark.parametrize("p", [3, 4, 5, 6, 7, 10, 12, 13, 15])
+def test_mixed_variants_agree(p, variant):
+    """Mixed form: the pipelined kernel (packed FP32 line contractions at
+    p = 3, 7, 10-15, its own FP32 line layouts at p = 5-7) and the
+    one-tile-per-block kernel (scalar lines below p = 13) give the same bits."""
+    dims, nstep = ((4, 3, 5) if p <= 7 else (2, 3, 2)), 10
     ops, mesh, omesh, (q, u, v, w) = case(p, dims)
-    dt = 0.1 / 5 / 64
+    dt = 0.1 / dims[2] / (p + 1) ** 2
     res = []
     for var in (sdg.VARIANT_BLOCK, variant):
         h = sdg.Handle(ops, mesh, sdg.FLAG_MIXED)
