@@ -289,17 +289,19 @@ struct Pair2<float> {
 // compute-type words).  x faces (+x = 2, -x = 4): q and u in two arrays,
 // entry (face, k, j) at XOFF*[face is -x] + Nq*k + j, the -x block shifted
 // by Nq^2 + 4 so that the eight writers of one k (a = 0 or Nq-1) hit
-// distinct banks; each x-face flux later replaces its q entry.  y faces
-// (-y = 1, +y = 3): (q, v) pairs, face-major, node a + Nq*k; the pair of
-// -y at node t is later replaced by the (flux -y, flux +y) pair.  Each
+// distinct banks.  y faces (-y = 1, +y = 3): (q, v) pairs, face-major, node
+// a + Nq*k.  After the flux phase the pair of -y at node t holds
+// (flux -y, flux +y) and the pair of +y at node t (flux +x, flux -x), so the
+// lift reads two pairs per node.  Each
 // scalar store of a warp then costs two wavefronts (one per half-warp), and
 // a pair store of the y writers one (they fill one quarter-warp).
 //
 // The split x arrays pay off where a pair is 16 bytes (FP64, whose 128-bit
 // shared accesses run in quarter-warp phases: the x writers span all four).
 // With 8-byte FP32 pairs the x faces keep (q, u) pairs like the y faces
-// (SPLIT = false): face +x at node j + Nq*k, -x at Nq^2 on, and the pair of
-// +x at node t later holds (flux +x, flux -x).
+// (SPLIT = false), face-major in the order -y, +x, +y, -x; after the flux
+// phase the pair of -y at node t holds (flux -y, flux +y) and the pair of +x
+// (flux +x, flux -x).
 template <int NQ, bool SPLIT>
 struct FaceArea {
   static constexpr int NQ2 = NQ * NQ;
@@ -504,13 +506,11 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
   constexpr bool XSPLIT = sizeof(TC) == 8;
   using FA = FaceArea<NQ, XSPLIT>;
   TC* fa = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT) + s * FA::ELEM;
-  TC* xq = fa;                                     // split x faces: q, then the flux
+  TC* xq = fa;                                     // split x faces: q
   TC* xu = fa + FA::XA;                            // split x faces: u
   V2* ypair = reinterpret_cast<V2*>(fa + FA::Y0);  // y faces: (q, v) pairs
-  // FP32: [4][NQ2] (q, un) pairs of the four faces, face-major; each face
-  // flux replaces the q of its pair, read by the lift at stride 2 (fQ).
+  // FP32: [4][NQ2] (q, un) pairs of the four faces, face-major.
   V2* fM = reinterpret_cast<V2*>(fa);
-  TC* fQ = fa;
 
   // Producer: one thread fills ring slot `slot` with tile `tile`.
   auto issue = [&](int tile, int slot) {
@@ -825,16 +825,24 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         const TC f2 = upwind_flux<AR, TC>(xq[xn], xu[xn], qP[1], unP[1], TC(1), sfs[1]);
         const TC f4 = upwind_flux<AR, TC>(xq[FA::XOFF + xn], xu[FA::XOFF + xn], qP[3],
                                           unP[3], TC(-1), sfs[3]);
-        xq[xn] = f2;
-        xq[FA::XOFF + xn] = f4;
+        // The fluxes go to the two y pairs of node t, which only this thread
+        // reads in this phase: (f1, f3) for the y faces, (f2, f4) for the x
+        // faces, one 16-byte read each per node in the epilogue.
         ypair[t] = V2{f1, f3};
+        ypair[NQ2 + t] = V2{f2, f4};
       } else {
+        // Fluxes as two pairs in the slots of faces 1 and 2 of node t (only
+        // this thread reads node t's minus sides in this phase): (f1, f3)
+        // for the y faces, (f2, f4) for the x faces.
+        TC fl[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
           const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
           const V2 m = fM[f * NQ2 + t];
-          fQ[2 * (f * NQ2 + t)] = upwind_flux<AR, TC>(m.x, m.y, qP[f], unP[f], sg, sfs[f]);
+          fl[f] = upwind_flux<AR, TC>(m.x, m.y, qP[f], unP[f], sg, sfs[f]);
         }
+        fM[t] = V2{fl[0], fl[2]};
+        fM[NQ2 + t] = V2{fl[1], fl[3]};
         qlo = static_cast<TC>(sq[t]);
         qhi = static_cast<TC>(sq[t + NQ2 * (NQ - 1)]);
       }
@@ -880,21 +888,12 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           for (int f = 0; f < 6; ++f) L[f] = ldro(A.lift + t + NQ2 * k + NP * f);
         }
         // tensorprod_Lift_hexahedral (kern:278-283): face order 1..6; the
-        // x/y face fluxes sit at stride 2 (the .x of each (q, un) pair).
-        // Face fluxes: 1, 3 at (i,k) = (a,k), 2, 4 at (j,k) = (b,k).
-        TC fl1, fl2, fl3, fl4;
-        if constexpr (XSPLIT) {
-          const V2 fyk = ypair[a + NQ * k];
-          fl1 = fyk.x;
-          fl3 = fyk.y;
-          fl2 = xq[b + NQ * k];
-          fl4 = xq[FA::XOFF + b + NQ * k];
-        } else {
-          fl1 = fQ[2 * (0 * NQ2 + a + NQ * k)];
-          fl2 = fQ[2 * (1 * NQ2 + b + NQ * k)];
-          fl3 = fQ[2 * (2 * NQ2 + a + NQ * k)];
-          fl4 = fQ[2 * (3 * NQ2 + b + NQ * k)];
-        }
+        // x/y face fluxes as (f1, f3) at (i,k) = (a,k) and (f2, f4) at
+        // (j,k) = (b,k).
+        const V2* fp = XSPLIT ? ypair : fM;
+        const V2 f13 = fp[a + NQ * k];
+        const V2 f24 = fp[NQ2 + b + NQ * k];
+        const TC fl1 = f13.x, fl3 = f13.y, fl2 = f24.x, fl4 = f24.y;
         TC lf = AR::mul(L[0], fl1);
         lf = AR::mad(L[1], fl2, lf);
         lf = AR::mad(L[2], fl3, lf);
