@@ -58,7 +58,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="fp64_32c_p7",
-                    choices=sorted(WORKLOADS) + ["batch_fp64", "batch_mixed", "served"])
+                    choices=sorted(WORKLOADS) + ["batch_fp64", "batch_mixed", "served",
+                                                 "divlike_var5_32c_p7"])
     ap.add_argument("--requests", type=int, default=200,
                     help="served workload: number of requests in the stream")
     ap.add_argument("--seq-sample", type=int, default=12,
@@ -141,7 +142,8 @@ def measured_peaks():
 def profiled_traffic(workload):
     """Per-launch DRAM bytes of the fused stage kernel from the committed ncu
     summary (profiles/<kernel>_<workload>.json), or None."""
-    path = os.path.join(REPO, "profiles", f"tend_stage_{workload}.json")
+    name = workload if workload.startswith("divlike") else f"tend_stage_{workload}"
+    path = os.path.join(REPO, "profiles", f"{name}.json")
     if os.path.exists(path):
         with open(path) as f:
             return json.load(f).get("dram_bytes_per_launch")
@@ -527,6 +529,124 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_derivative(args):
+    """divlike_var5_32c_p7: the five-field derivative operator
+    (sdg_divlike_dev, element_operation_kernel_matvec_divlike_dirXYZ_var5_P<p>)
+    on 32^3 elements at p = 7, FMA form, seeded random fields.  A step is one
+    call: the x-, y- and z-derivatives of 5 x 16.8 M field values, read from
+    three input arrays and written to three outputs (4.0 GB in all, no L2
+    flush needed).  Metric: field values differentiated per second (each gets
+    its three derivatives).  e2e: the same call with the inputs copied from
+    pinned host memory and the outputs read back every step."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
+    import sdg_b200 as sdg
+    p, nvar, NeX = 7, 5, 32
+    Ne = NeX ** 3
+    ops = sdg.read_operators(p)
+    Np = (p + 1) ** 3
+    n = Ne * nvar * Np
+    gen = torch.Generator(device="cuda").manual_seed(7 + rank)
+    ins = [torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) for _ in range(3)]
+    outs = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(3)]
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def call():
+        sdg.divlike_dirXYZ_var_dev(ops.D1D, nvar, Ne, *ins, *outs, flags=0, stream=sp)
+
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    gpu_idx = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            gpu_idx = int(vis.split(",")[local])
+        except ValueError:
+            pass
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_idx) as clk:
+        rep.barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            call()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        rep.barrier()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    t_max = rep.max(t)
+    value = world * n * args.steps / t_max
+    bytes_per_value = 6 * 8  # three inputs read, three outputs written
+    achieved = n * bytes_per_value / (t / args.steps) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic(args.workload)
+
+    # e2e: host inputs in, host outputs back, every step
+    n_e2e = max(3, min(10, args.steps // 20))
+    h_in = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    h_out = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    for hi, di in zip(h_in, ins):
+        hi.copy_(di)
+    torch.cuda.synchronize()
+    rep.barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        for hi, di in zip(h_in, ins):
+            di.copy_(hi, non_blocking=True)
+        call()
+        for ho, do in zip(h_out, outs):
+            ho.copy_(do, non_blocking=True)
+        torch.cuda.synchronize()
+    t_e2e = rep.max(time.perf_counter() - t0)
+    e2e = world * n * n_e2e / t_e2e
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import orc
+        ne_s = 2048  # sample: 1/16 of the elements
+        m = ne_s * nvar * Np
+        xs = [ins[k][:m].cpu().numpy() for k in range(3)]
+        orc.divlike_fields(orc.OPT1, ops.D1D, nvar, ne_s, *xs)
+        k, t0 = 0, time.perf_counter()
+        while True:
+            orc.divlike_fields(orc.OPT1, ops.D1D, nvar, ne_s, *xs)
+            k += 1
+            el = time.perf_counter() - t0
+            if el > args.cpu_seconds or k >= 200:
+                break
+        cpu = {"value": m * k / el, "unit": "field values/s", "cores": orc.num_threads(),
+               "kind": "port",
+               "sample": f"{k} calls on {ne_s} of the {Ne} elements (OPT1 order), {el:.1f} s"}
+    rep.close()
+    if rank != 0:
+        return
+    line = {"metric": "field values differentiated/s (x, y, z derivatives each)",
+            "value": value, "unit": "field values/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded normal fields)",
+            "config": {"workload": args.workload, "mesh": [NeX, NeX, NeX], "p": p,
+                       "fields_per_element": nvar, "values_per_gpu": n,
+                       "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic": traffic, "kernel": "derivative_kernel (sdg_divlike_dev)",
+                         "alg_bytes_per_value": bytes_per_value},
+            "e2e": {"value": e2e, "unit": "field values/s", "h2d_bytes_per_step": 3 * n * 8,
+                    "d2h_bytes_per_step": 3 * n * 8,
+                    "api": "host-to-device copies + sdg_divlike_dev + device-to-host copies"},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps}
+    print(json.dumps(line), flush=True)
+
+
 def run_served(args):
     """Served request stream: Poisson arrivals at ~80% load; Ne/axis
     U{8..32}, p U{3..11}, nstep U{50..400}, FP32/FP64 flag.  The stream is
@@ -618,6 +738,8 @@ def main():
         run_batch(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "divlike_var5_32c_p7":
+        run_derivative(args)
     else:
         run_ours(args)
 

@@ -286,6 +286,39 @@ int sdg_serve_stats(sdg_server* s, double* out4);
 /* Stops the worker and frees everything. */
 int sdg_serve_destroy(sdg_server* s);
 
+/* Sum-factorised x-, y- and z-derivatives of nvar fields per element, on
+ * device arrays, asynchronously on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream).  Replaces
+ * element_operation_kernel_matvec_divlike_dirXYZ_var5_P<p>
+ * (mod_dg_optr_kernel_opt1.F90.erb:347-465; nvar = 5 there, any nvar >= 1
+ * here): out_x(i,j,k) = sum_l D(i,l) in_x(l,j,k), out_y(i,j,k) =
+ * sum_l in_y(i,l,k) D(j,l), out_z(i,j,k) = sum_l in_z(i,j,l) D(k,l), per
+ * element and field.  Arrays hold element e, field v, node
+ * n = i + Nq*j + Nq^2*k at n + Np*(v + nvar*e) (the reference's per-element
+ * vec_in_x(np, np^2*5) stacked over elements); D1D is the host (Nq,Nq)
+ * column-major matrix of operator_data.  flags: 0 (FMA, OPT1 order),
+ * SDG_FLAG_EXACT (every product and sum rounded, OPT1 order: bit-exact with
+ * the reference routine), SDG_FLAG_EXACT | SDG_FLAG_ORDER_GENERAL
+ * (mod_dg_optr_kernel.f90:197-258 order).  Outputs must not overlap the
+ * inputs.  The reference's y output index (erb:400) overruns its array for
+ * kv >= 3; this computes the derivative that routine is written for.
+ * Nq = 2..16; SDG_ERR_ARG on bad sizes, flags or null arrays. */
+int sdg_divlike_dev(int Nq, int nvar, long long Ne, const double* D1D,
+                    const double* in_x, const double* in_y, const double* in_z,
+                    double* out_x, double* out_y, double* out_z, int flags,
+                    void* stream);
+
+/* The x-, y- and z-derivatives of one field per element (layout as above with
+ * nvar = 1), reading the input once.  Replaces
+ * element_operation_kernel_matvec_gradlike_dirXYZ_P<p>
+ * (mod_dg_optr_kernel_opt1.F90.erb:166-219); the z-derivative's first term
+ * reads vec_in(i,j,1)*Mat_tr(1,k) like its other terms (the reference text
+ * has vec_in(i,1,k)*Mat_tr(1,j) there, erb:209).  Flags and errors as
+ * sdg_divlike_dev. */
+int sdg_gradlike_dev(int Nq, long long Ne, const double* D1D, const double* in,
+                     double* out_x, double* out_y, double* out_z, int flags,
+                     void* stream);
+
 /* min and max of n doubles at device pointer q, written to the device
  * pointer out2 (out2[0] = min, out2[1] = max), asynchronously on `stream`
  * (a cudaStream_t; NULL = the legacy default stream).  No counterpart in the

@@ -36,6 +36,7 @@ _SIGS = {
     "orc_init_fields": (_I, [_I, _U64, _I, _D, _D, _D, _P, _I, _I, _I, _P, _P, _P, _P]),
     "orc_random_velocity": (None, [_U64, _P]),
     "orc_num_threads": (_I, []),
+    "orc_divlike_fields": (_I, [_I, _I, _I, ctypes.c_longlong, _P, _P, _P, _P, _P, _P, _P]),
 }
 
 _lib = None
@@ -169,3 +170,18 @@ def run_rk3(evaltype, q, u, v, w, ops, mesh, dt, nstep, output_interval=0):
 
 def num_threads():
     return int(lib().orc_num_threads())
+
+
+def divlike_fields(evaltype, D1D, nvar, Ne, ix, iy, iz):
+    """divlike_dirXYZ_var5 / gradlike_dirXYZ restated (sdg_oracle.h): arrays of
+    Ne*nvar*Np values, unit (element e, field v) at Np*(v + nvar*e); returns
+    (ox, oy, oz)."""
+    D = np.asarray(D1D, dtype=np.float64, order="F")
+    Nq = D.shape[0]
+    ix, iy, iz = (np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (ix, iy, iz))
+    outs = [np.empty_like(ix) for _ in range(3)]
+    rc = lib().orc_divlike_fields(evaltype, Nq, nvar, Ne, _p(D), _p(ix), _p(iy), _p(iz),
+                                  *[_p(o) for o in outs])
+    if rc:
+        raise ValueError(f"oracle: divlike_fields failed ({rc})")
+    return tuple(outs)

@@ -493,6 +493,29 @@ int orc_cal_tend(int evaltype, double* dqdt, const double* q, const double* u,
   return 0;
 }
 
+int orc_divlike_fields(int evaltype, int Nq, int nvar, long long Ne,
+                       const double* D1D, const double* ix, const double* iy,
+                       const double* iz, double* ox, double* oy, double* oz) {
+  if (Nq < 2 || Nq > 16 || nvar < 1 || Ne < 0) return 1;
+  if (evaltype != ORC_GENERAL && evaltype != ORC_OPT1) return 1;
+  // D1D_tr = transpose(D1D) (mod_mesh.f90:263).
+  std::vector<double> Dtr(static_cast<size_t>(Nq) * Nq);
+  for (int i = 0; i < Nq; ++i)
+    for (int l = 0; l < Nq; ++l) Dtr[l + Nq * i] = D1D[i + Nq * l];
+  const long long Np = static_cast<long long>(Nq) * Nq * Nq;
+  const long long units = Ne * nvar;
+  opt1_fn opt1 = opt1_table(Nq);
+#pragma omp parallel for schedule(static)
+  for (long long u = 0; u < units; ++u) {
+    const long long o = u * Np;
+    if (evaltype == ORC_OPT1)
+      opt1(ox + o, oy + o, oz + o, D1D, Dtr.data(), ix + o, iy + o, iz + o);
+    else
+      divlike_general(ox + o, oy + o, oz + o, D1D, Dtr.data(), ix + o, iy + o, iz + o, Nq);
+  }
+  return 0;
+}
+
 int orc_run_rk3(int evaltype, double* q, const double* u, const double* v,
                 const double* w, const double* D1D, const double* Lift_mat,
                 const int* VMapM, const int* VMapP, const int* halo_src_map,

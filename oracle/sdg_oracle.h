@@ -95,6 +95,21 @@ void orc_random_velocity(unsigned long long seed, double* vel3);
 /* Number of OpenMP threads the oracle will use. */
 int orc_num_threads(void);
 
+/* element_operation_kernel_matvec_divlike_dirXYZ_var5_P<p>
+ * (mod_dg_optr_kernel_opt1.F90.erb:347-465) over Ne elements of nvar fields:
+ * for each (element, field) unit of Np nodes at offset Np*(v + nvar*e),
+ * ox/oy/oz = the x/y/z contraction of ix/iy/iz with D1D, in the OPT1 order
+ * (the same per-direction sums as divlike_dirXYZ_P<p>, erb:228-344) or the
+ * GENERAL order (mod_dg_optr_kernel.f90:197-258).  With ix = iy = iz and
+ * nvar = 1 this is element_operation_kernel_matvec_gradlike_dirXYZ_P<p>
+ * (erb:166-219).  It computes what those routines are written for: the var5
+ * y output index of erb:400 and the gradlike z first term of erb:209 are
+ * index slips in the reference text (out-of-range and transposed indices),
+ * not reproduced.  Returns 0, or 1 on bad sizes or evaltype. */
+int orc_divlike_fields(int evaltype, int Nq, int nvar, long long Ne,
+                       const double* D1D, const double* ix, const double* iy,
+                       const double* iz, double* ox, double* oy, double* oz);
+
 #ifdef __cplusplus
 }
 #endif

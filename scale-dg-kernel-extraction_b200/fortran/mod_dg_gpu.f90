@@ -28,6 +28,7 @@ module mod_dg_gpu
   public :: dg_gpu_setup, dg_gpu_finalize, dg_gpu_cal_tend
   public :: dg_gpu_set_state, dg_gpu_get_state, dg_gpu_rk3_steps, dg_gpu_minmax
   public :: SDG_FLAG_EXACT, SDG_FLAG_ORDER_GENERAL, SDG_FLAG_MIXED
+  public :: sdg_divlike_dev, sdg_gradlike_dev
 
   integer(c_int), parameter :: SDG_FLAG_EXACT = 1
   integer(c_int), parameter :: SDG_FLAG_ORDER_GENERAL = 2
@@ -84,6 +85,33 @@ module mod_dg_gpu
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: h
       real(c_double), intent(out) :: qmin, qmax
+    end function
+    !> x-, y- and z-derivatives of nvar fields per element, on device arrays
+    !! (addresses from, e.g., an OpenACC host_data use_device region); replaces
+    !! element_operation_kernel_matvec_divlike_dirXYZ_var5_P<p>
+    !! (mod_dg_optr_kernel_opt1.F90.erb:347-465) over all elements at once.
+    !! Array layout: vec_in_x(Np, nvar) of each element, stacked over elements.
+    integer(c_int) function sdg_divlike_dev(Nq, nvar, Ne, D1D, in_x, in_y, in_z, &
+        out_x, out_y, out_z, flags, stream) bind(C, name="sdg_divlike_dev")
+      import :: c_int, c_long_long, c_double, c_ptr
+      integer(c_int), value :: Nq, nvar
+      integer(c_long_long), value :: Ne
+      real(c_double), intent(in) :: D1D(*)
+      type(c_ptr), value :: in_x, in_y, in_z, out_x, out_y, out_z
+      integer(c_int), value :: flags
+      type(c_ptr), value :: stream
+    end function
+    !> The three derivatives of one field per element; replaces
+    !! element_operation_kernel_matvec_gradlike_dirXYZ_P<p> (erb:166-219).
+    integer(c_int) function sdg_gradlike_dev(Nq, Ne, D1D, vec_in, out_x, out_y, out_z, &
+        flags, stream) bind(C, name="sdg_gradlike_dev")
+      import :: c_int, c_long_long, c_double, c_ptr
+      integer(c_int), value :: Nq
+      integer(c_long_long), value :: Ne
+      real(c_double), intent(in) :: D1D(*)
+      type(c_ptr), value :: vec_in, out_x, out_y, out_z
+      integer(c_int), value :: flags
+      type(c_ptr), value :: stream
     end function
   end interface
 

@@ -78,6 +78,8 @@ SIGNATURES = {
     "sdg_launch_count": (_LL, [_P]),
     "sdg_set_kernel_variant": (_I, [_P, _I]),
     "sdg_minmax_dev_noalloc": (_I, [_P, _LL, _P, _P]),
+    "sdg_divlike_dev": (_I, [_I, _I, _LL, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "sdg_gradlike_dev": (_I, [_I, _LL, _P, _P, _P, _P, _P, _I, _P]),
     "sdg_batch_create": (_I, [ctypes.POINTER(_P), _I]),
     "sdg_batch_add": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _D,
                            ctypes.POINTER(_I)]),
@@ -413,6 +415,31 @@ def advect3d_eq_cal_tend(dqdt, q, u, v, w, D1D, D1D_tr, Lift_mat, VMapM, VMapP,
     out = h.cal_tend(q, u, v, w)
     dqdt[:, :Ne] = out[:, :Ne]
     return dqdt
+
+
+def divlike_dirXYZ_var_dev(D1D, nvar, Ne, in_x, in_y, in_z, out_x, out_y, out_z, flags=0,
+                           stream=None):
+    """element_operation_kernel_matvec_divlike_dirXYZ_var5_P<p>
+    (mod_dg_optr_kernel_opt1.F90.erb:347-465) on device tensors.
+
+    The arrays (anything with data_ptr(), float64, contiguous) hold element
+    e, field v, node n = i + Nq*j + Nq^2*k at n + Np*(v + nvar*e); out_d
+    receives the d-derivative of in_d.  D1D is the (Nq,Nq) operator matrix.
+    flags: 0, FLAG_EXACT, or FLAG_EXACT | FLAG_ORDER_GENERAL."""
+    D = _f64(D1D)
+    _check(lib().sdg_divlike_dev(D.shape[0], nvar, Ne, _p(D), in_x.data_ptr(), in_y.data_ptr(),
+                                 in_z.data_ptr(), out_x.data_ptr(), out_y.data_ptr(),
+                                 out_z.data_ptr(), flags, stream))
+
+
+def gradlike_dirXYZ_dev(D1D, Ne, vec_in, out_x, out_y, out_z, flags=0, stream=None):
+    """element_operation_kernel_matvec_gradlike_dirXYZ_P<p>
+    (mod_dg_optr_kernel_opt1.F90.erb:166-219) on device tensors: the x-, y-
+    and z-derivatives of one field (layout as divlike_dirXYZ_var_dev with
+    nvar = 1)."""
+    D = _f64(D1D)
+    _check(lib().sdg_gradlike_dev(D.shape[0], Ne, _p(D), vec_in.data_ptr(), out_x.data_ptr(),
+                                  out_y.data_ptr(), out_z.data_ptr(), flags, stream))
 
 
 class Problem:

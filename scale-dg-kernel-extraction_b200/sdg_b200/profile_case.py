@@ -25,7 +25,12 @@ def main():
     ap.add_argument("--mode", default="GPU", choices=["GPU", "OPT1", "GENERAL", "MIXED"])
     ap.add_argument("--warm", type=int, default=2, help="RK3 steps before the launches")
     ap.add_argument("--launches", type=int, default=3)
+    ap.add_argument("--op", default="stage", choices=["stage", "divlike"],
+                    help="stage: fused RK stage kernels; divlike: the five-field "
+                         "derivative operator (sdg_divlike_dev) on the same mesh")
     a = ap.parse_args()
+    if a.op == "divlike":
+        return divlike_case(a)
     flags = {"GPU": 0, "OPT1": sdg.FLAG_EXACT,
              "GENERAL": sdg.FLAG_EXACT | sdg.FLAG_ORDER_GENERAL,
              "MIXED": sdg.FLAG_MIXED}[a.mode]
@@ -44,6 +49,24 @@ def main():
     mn, mx = h.minmax()
     h.close()
     print(f"profile_case done: {a.mesh}^3 p={a.p} {a.mode}, min {mn:.6e} max {mx:.6e}")
+
+
+def divlike_case(a):
+    """--warm + --launches calls of sdg_divlike_dev (five seeded fields per
+    element of a mesh^3 box at order p, FMA form)."""
+    import torch
+    nvar = 5
+    ops = sdg.read_operators(a.p)
+    Ne = a.mesh ** 3
+    n = Ne * nvar * (a.p + 1) ** 3
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    ins = [torch.randn(n, dtype=torch.float64, device="cuda", generator=gen) for _ in range(3)]
+    outs = [torch.empty_like(ins[0]) for _ in range(3)]
+    for _ in range(a.warm + a.launches):
+        sdg.divlike_dirXYZ_var_dev(ops.D1D, nvar, Ne, *ins, *outs)
+    torch.cuda.synchronize()
+    print(f"profile_case done: divlike {a.mesh}^3 p={a.p} x{nvar}, "
+          f"|out_x| max {float(outs[0].abs().max()):.6e}")
 
 
 if __name__ == "__main__":

@@ -155,6 +155,39 @@ def test_ensemble_argument_errors():
     assert e.value.code == sdg.SDG_ERR_ARG
 
 
+def test_derivative_operator_argument_errors():
+    """sdg_divlike_dev / sdg_gradlike_dev check sizes, flags and arrays before
+    touching a device."""
+    import ctypes
+    L = sdg.lib()
+    D = np.eye(4, order="F")
+    dp = ctypes.c_void_p(D.ctypes.data)
+    one = ctypes.c_void_p(8)  # never dereferenced: every call below fails first
+    def div(Nq=4, nvar=5, Ne=2, flags=0, arr=one, d=dp):
+        return L.sdg_divlike_dev(Nq, nvar, Ne, d, arr, arr, arr, arr, arr, arr, flags, None)
+    assert div(Nq=1) == sdg.SDG_ERR_ARG
+    assert div(Nq=17) == sdg.SDG_ERR_ARG
+    assert div(nvar=0) == sdg.SDG_ERR_ARG
+    assert div(Ne=-1) == sdg.SDG_ERR_ARG
+    assert div(flags=sdg.FLAG_MIXED) == sdg.SDG_ERR_ARG
+    assert div(flags=sdg.FLAG_ORDER_GENERAL) == sdg.SDG_ERR_ARG
+    assert div(arr=None) == sdg.SDG_ERR_ARG
+    assert div(d=None) == sdg.SDG_ERR_ARG
+    assert L.sdg_gradlike_dev(4, 2, dp, None, one, one, one, 0, None) == sdg.SDG_ERR_ARG
+    assert L.sdg_gradlike_dev(0, 2, dp, one, one, one, one, 0, None) == sdg.SDG_ERR_ARG
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_derivative_operators_fail_loudly_without_device():
+    import ctypes
+    D = np.eye(4, order="F")
+    a = np.zeros(64 * 2)
+    pa = ctypes.c_void_p(a.ctypes.data)
+    rc = sdg.lib().sdg_gradlike_dev(4, 2, ctypes.c_void_p(D.ctypes.data), pa, pa, pa, pa, 0,
+                                    None)
+    assert rc == sdg.SDG_ERR_CUDA
+
+
 def test_evaltype_selector():
     with pytest.raises(sdg.SdgError):
         sdg.dg_optr_kernel_setup("FASTEST")

@@ -133,3 +133,45 @@ def test_rk3_reference_run_shape():
     assert np.array_equal(diag[:, 0], np.arange(100, 1001, 100))
     assert np.all(np.abs(diag[:, 1:]) <= 1.0 + 1e-6)
     assert np.all(diag[:, 1] < -0.99) and np.all(diag[:, 2] > 0.99)
+
+
+@pytest.mark.parametrize("p", [1, 3, 7, 8, 12, 15])
+def test_divlike_fields_known_answers(p):
+    """divlike_dirXYZ_var5 / gradlike_dirXYZ restated: on LGL nodes the
+    derivative matrix differentiates polynomials of degree <= p exactly, so
+    f = x^a y^b z^c (a, b, c <= p) has derivatives a x^(a-1) y^b z^c etc.
+    Each of nvar fields per element gets its own exponents; GENERAL and OPT1
+    agree to rounding (bit for bit for p <= 7)."""
+    ops = orc.read_operators(p)
+    Nq = p + 1
+    x = ops.x1D
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")  # node (i,j,k)
+    nvar, Ne = 3, 4
+    rng = np.random.default_rng(p)
+    ins, want = [], []
+    for e in range(Ne):
+        for v in range(nvar):
+            a_, b_, c_ = rng.integers(0, p + 1, size=3)
+            f = X ** a_ * Y ** b_ * Z ** c_
+            dx = a_ * X ** max(a_ - 1, 0) * Y ** b_ * Z ** c_
+            dy = b_ * X ** a_ * Y ** max(b_ - 1, 0) * Z ** c_
+            dz = c_ * X ** a_ * Y ** b_ * Z ** max(c_ - 1, 0)
+            # node n = i + Nq*j + Nq^2*k: Fortran order of the (i,j,k) grid
+            ins.append(f.ravel(order="F"))
+            want.append([d.ravel(order="F") for d in (dx, dy, dz)])
+    f = np.concatenate(ins)
+    outs = {}
+    for ev in (orc.OPT1, orc.GENERAL):
+        outs[ev] = orc.divlike_fields(ev, ops.D1D, nvar, Ne, f, f, f)
+        for d in range(3):
+            ref = np.concatenate([w[d] for w in want])
+            assert np.max(np.abs(outs[ev][d] - ref)) <= 1e-10 * max(1.0, np.max(np.abs(ref)))
+    for d in range(3):
+        if p <= 7:
+            assert np.array_equal(outs[orc.OPT1][d], outs[orc.GENERAL][d])
+        else:
+            assert rel_maxnorm(outs[orc.OPT1][d], outs[orc.GENERAL][d]) < 1e-13
+    # separate inputs per direction: out_d depends on in_d only
+    zero = np.zeros_like(f)
+    ox, oy, oz = orc.divlike_fields(orc.OPT1, ops.D1D, nvar, Ne, f, zero, zero)
+    assert np.array_equal(ox, outs[orc.OPT1][0]) and not oy.any() and not oz.any()
