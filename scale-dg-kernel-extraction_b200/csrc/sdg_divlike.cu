@@ -31,8 +31,9 @@
 // registers and puts the x and y inputs into shared line buffers in the
 // layouts of the tendency kernel (LineIdx, conflict-free at p = 3, 5-9);
 // after a barrier it contracts its x-line (j,k) = (a,b) and y-line
-// (i,k) = (a,b) in place and its z-column in registers, and after a second
-// barrier it stores its columns of the three outputs.  No scratch, no
+// (i,k) = (a,b) in place and its z-column in registers (at some orders the
+// z-column first, before the barrier), and after a second barrier it stores
+// its x and y output columns.  No scratch, no
 // atomics: every unit reads and writes only its own Np nodes.
 #include <cuda_runtime.h>
 
@@ -68,7 +69,23 @@ __global__ void __launch_bounds__((Geo<NQ>::THREADS + 31) / 32 * 32)
   const long long base = u * NP + t;
 
   // Column (a,b) of the three inputs; with one input for all three
-  // directions (gradlike) it is read once.
+  // directions (gradlike) it is read once.  The z-derivative needs only this
+  // thread's column.  Where registers are tight it is done before the
+  // barrier, so that the column leaves the registers before the line
+  // contractions; elsewhere after the lines, which hides the column loads
+  // behind the barrier.  Measured per order (G values/s, early / late z):
+  // gradlike p = 8 149 / 126, p = 9 148 / 118; both operators p = 10-12
+  // 109-146 / 93-133; five fields p = 7 125 / 144, p = 8 115 / 125, p = 9
+  // 112 / 119; both p = 14 76-81 / 135-155.
+  constexpr bool EARLYZ = (NQ >= 11 && NQ <= 13) || (ONE && (NQ == 9 || NQ == 10));
+  auto zderiv = [&](const double (&col)[NQ]) {
+    // Z-dir (erb:430-463): vec_in_z(i,j,l) * Mat_tr(l,k), stored straight
+    // from registers (coalesced over the warp).
+#pragma unroll
+    for (int k = 0; k < NQ; ++k)
+      oz[base + NQ2 * k] = contract<NQ, ORDER, AR, double>(
+          [&](int l) { return col[l]; }, [&](int l) { return D.d[k * NQ + l]; });
+  };
   double col[NQ];
   if (active) {
 #pragma unroll
@@ -78,6 +95,7 @@ __global__ void __launch_bounds__((Geo<NQ>::THREADS + 31) / 32 * 32)
       sY[LI::coly(a, b, k)] = ONE ? xv : ldro(iy + base + NQ2 * k);
       col[k] = ONE ? xv : ldro(iz + base + NQ2 * k);
     }
+    if constexpr (EARLYZ) zderiv(col);
   }
   __syncthreads();
   if (active) {
@@ -97,12 +115,7 @@ __global__ void __launch_bounds__((Geo<NQ>::THREADS + 31) / 32 * 32)
     for (int j = 0; j < NQ; ++j)
       sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, double>(
           [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
-    // Z-dir (erb:430-463): vec_in_z(i,j,l) * Mat_tr(l,k), stored straight
-    // from registers (coalesced over the warp).
-#pragma unroll
-    for (int k = 0; k < NQ; ++k)
-      oz[base + NQ2 * k] = contract<NQ, ORDER, AR, double>(
-          [&](int l) { return col[l]; }, [&](int l) { return D.d[k * NQ + l]; });
+    if constexpr (!EARLYZ) zderiv(col);
   }
   __syncthreads();
   if (active) {
