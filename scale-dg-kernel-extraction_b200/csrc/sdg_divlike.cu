@@ -39,6 +39,7 @@
 
 #include "sdg_gpu.h"
 #include "sdg_internal.h"
+#include "sdg_launch.h"
 #include "sdg_tend.cuh"
 #include "sdg_tend_pipe.cuh"
 
@@ -144,15 +145,17 @@ int launch_derivative(const DerivCall& c) {
   using G = Geo<NQ>;
   auto kern = derivative_kernel<NQ, EXACT, ORDER, ONE>;
   const size_t smem = sizeof(double) * 2 * LineIdx<NQ, 8>::SIZE * G::EPB;
-  static bool attr_done = false;  // per instantiation
-  if (!attr_done) {
+  static DeviceSetup setup;  // per instantiation and device
+  const int dev = setup_device();
+  if (dev < 0) return fail(SDG_ERR_CUDA, "derivative: no usable current device");
+  if (setup.slot[dev].load(std::memory_order_relaxed) == 0) {
     if (smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            static_cast<int>(smem));
       if (e != cudaSuccess)
         return fail(SDG_ERR_CUDA, "derivative kernel set-up failed: %s", cudaGetErrorString(e));
     }
-    attr_done = true;
+    setup.slot[dev].store(1, std::memory_order_relaxed);
   }
   if (c.units <= 0) return SDG_OK;
   DMat<NQ, double> d;

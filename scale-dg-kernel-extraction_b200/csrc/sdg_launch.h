@@ -4,7 +4,25 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 namespace sdg {
+
+// Per-device cache of a kernel's one-time launch set-up: function
+// attributes and occupancy queries act on the current device only, so a
+// process that drives several devices sets each one up.  One static
+// instance per kernel instantiation; a slot holds 0 until set up.
+constexpr int kMaxSetupDevices = 64;
+struct DeviceSetup {
+  std::atomic<int> slot[kMaxSetupDevices];
+};
+
+// The current device, or -1 when it cannot be read or lies beyond the cache.
+inline int setup_device() {
+  int d = -1;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxSetupDevices) return -1;
+  return d;
+}
 
 // Summation order of the contractions for NQ > 8: OPT1's three partial sums
 // (mod_dg_optr_kernel_opt1.F90.erb:242-274) or GENERAL's sequential loop

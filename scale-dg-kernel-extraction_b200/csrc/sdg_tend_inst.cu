@@ -27,7 +27,10 @@ constexpr int NQ = SDG_NQ;
 template <auto KERN, typename Args, typename Dm>
 int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, const Dm& d) {
   constexpr auto kern = KERN;
-  static int blocks_per_sm = 0;  // per kernel; its plan is fixed
+  static DeviceSetup setup;  // blocks per SM, per kernel and device
+  const int dev = setup_device();
+  if (dev < 0) return static_cast<int>(cudaErrorInvalidDevice);
+  int blocks_per_sm = setup.slot[dev].load(std::memory_order_relaxed);
   if (blocks_per_sm == 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
@@ -37,6 +40,7 @@ int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, con
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, PipeGeo<NQ>::THREADS, smem);
     if (e != cudaSuccess) return static_cast<int>(e);
     blocks_per_sm = nb > 0 ? nb : 1;
+    setup.slot[dev].store(blocks_per_sm, std::memory_order_relaxed);
   }
   if (ntiles <= 0) return 0;
   const int grid = std::min(ntiles, blocks_per_sm * (s.num_sms > 0 ? s.num_sms : 148));
@@ -102,10 +106,12 @@ int run(const LaunchSpec& s) {
     // (64 registers per thread) with the largest shared-memory carveout.
     if (s.variant == kVariantBlockOcc) {
       auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, 8>;
-      static bool carve_done = false;
-      if (!carve_done) {
+      static DeviceSetup carve;  // per device
+      const int dev = setup_device();
+      if (dev < 0) return static_cast<int>(cudaErrorInvalidDevice);
+      if (carve.slot[dev].load(std::memory_order_relaxed) == 0) {
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        carve_done = true;
+        carve.slot[dev].store(1, std::memory_order_relaxed);
       }
       if (s.nelem <= 0) return 0;
       a.prefetch_dist = 8 * (s.num_sms > 0 ? s.num_sms : 148);
@@ -120,7 +126,10 @@ int run(const LaunchSpec& s) {
   // (p = 11: 29.5 -> 48.5 G DOF-updates/s, p = 15: 47.5 -> 53.0).
   constexpr int MB = (!EXACT && NQ >= 12) ? 2 : 1;
   auto kern = tend_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, MB>;
-  static int resident = 0;  // blocks per SM, per instantiation
+  static DeviceSetup setup;  // blocks per SM, per instantiation and device
+  const int dev = setup_device();
+  if (dev < 0) return static_cast<int>(cudaErrorInvalidDevice);
+  int resident = setup.slot[dev].load(std::memory_order_relaxed);
   if (resident == 0) {
     if (smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(
@@ -132,6 +141,7 @@ int run(const LaunchSpec& s) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::THREADS, smem);
     if (e != cudaSuccess) return static_cast<int>(e);
     resident = nb > 0 ? nb : 1;
+    setup.slot[dev].store(resident, std::memory_order_relaxed);
   }
   if (s.nelem <= 0) return 0;
   a.prefetch_dist = resident * (s.num_sms > 0 ? s.num_sms : 148);
