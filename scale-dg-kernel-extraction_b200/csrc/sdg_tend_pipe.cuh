@@ -151,7 +151,8 @@ __device__ __forceinline__ T ld_stream(const T* p) {
 //   p = 3: 78.2 -> 80.7 G with this one).  The same map is conflict-free for
 //   FP32 as well (elements 80 words apart, 16 mod 32), but its XOR
 //   addressing took the FP32 kernels from 96 to 111 registers and one
-//   resident block fewer: 101.5 against 104.0 G, so FP32 keeps the padding.
+//   resident block fewer: 101.5 against 104.0 G, so FP32 uses a skewed linear
+//   layout at Nq = 4 instead (SkewIdx below).
 template <int NQ, int WORD>
 struct LineIdx {
   static constexpr int SIZE = Geo<NQ>::SBUF;
@@ -214,13 +215,18 @@ struct SkewIdx {
 // +7 %, p = 9 +10 %.  FP32 (four-byte banks, 32-lane groups): Nq = 6
 // x = 36i + j + 6k, y = 38j + i + 6k (150 -> 114, ideal 96) and Nq = 7
 // x = 49k + i + 7j, y = 49j + k + 7i (168 -> 140, ideal 112); measured mixed
-// p = 5 +2 %, p = 6 +2 %.  Layouts that reached their ideal but measured no gain
+// p = 5 +2 %, p = 6 +2 %; Nq = 4 x = 20i + j + 4k, y = 20j + i + 4k (96 -> 64, its
+// ideal), mixed p = 3 +6 % (the XOR map of FP64 is conflict-free for four-byte
+// words too, but its addressing cost the FP32 kernel a resident block).  Layouts
+// that reached their ideal but measured no gain
 // were left out: FP64 Nq = 11 (429 -> 352; 66.6 against 67.6 G) and FP32
 // Nq = 10 (250 -> 190; 109.2 against 112.9 G).
 template <>
 struct LineIdx<6, 8> : SkewIdx<6, 0, 1, 2, 38, 1, 0, 2, 38, 228> {};
 template <>
 struct LineIdx<7, 8> : SkewIdx<7, 0, 2, 1, 49, 1, 2, 0, 49, 343> {};
+template <>
+struct LineIdx<4, 4> : SkewIdx<4, 0, 1, 2, 20, 1, 0, 2, 20, 80> {};
 template <>
 struct LineIdx<6, 4> : SkewIdx<6, 0, 1, 2, 36, 1, 0, 2, 38, 228> {};
 template <>
