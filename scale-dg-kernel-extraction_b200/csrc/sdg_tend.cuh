@@ -383,6 +383,15 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
     }
   }
 
+  // The element's face-neighbour row, needed after phase 1: loaded first so
+  // that phase 1 covers its latency and the gathers of phase 2 wait on one
+  // load, not two in a chain.
+  int pb[6];
+  if (active) {
+#pragma unroll
+    for (int f = 0; f < 6; ++f) pb[f] = ldro(A.pbase + 6 * static_cast<long>(e) + f);
+  }
+
   // ---- Phase 1: load the column, form the volume fluxes ------------------
   if (active) {
 #pragma unroll
@@ -412,7 +421,6 @@ __global__ void __launch_bounds__(Geo<NQ>::THREADS, MINB)
   TC f5 = TC(0), f6 = TC(0);
   if (active) {
     // ---- Phase 2a: flux on the x/y faces, face node fp = t ---------------
-    const int* pb = A.pbase + 6 * static_cast<long>(e);
     const TC* fs = A.fscale + 6 * static_cast<long>(e);
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
