@@ -87,8 +87,8 @@ int launch_tend(const LaunchSpec& s);
 
 // Kernel variants: the one-tile-per-block kernel (tend_kernel) and the
 // persistent bulk-copy pipelined kernel (tend_pipe_kernel); identical
-// arithmetic.  Auto picks the pipelined one when two blocks fit per SM and
-// every array is 16-byte aligned.
+// arithmetic.  Auto picks the pipelined one when its shared-memory plan fits
+// one block (kPipeMaxSmem) and every array is 16-byte aligned.
 // kVariantBlockOcc is the one-tile-per-block kernel built for eight resident
 // blocks per SM (p = 3..7; other orders use kVariantBlock).
 enum KernelVariant {
