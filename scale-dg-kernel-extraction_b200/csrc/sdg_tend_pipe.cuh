@@ -47,14 +47,15 @@ namespace sdg {
 
 constexpr int kStatusWaitTimeout = 1;
 constexpr unsigned kWaitSpins = 1u << 22;
-// Largest shared-memory plan the pipelined kernel is used with: one block of
-// it within the 227 KB a block may opt in to.  Plans above 110 KB run one
-// block per SM; its copy ring still overlaps the next tile's loads with
-// compute, which measured faster than the one-tile-per-block kernel there
-// (G DOF-updates/s, one-block pipelined / one tile per block: FP64 p = 12
-// 54.7 / 46.9, p = 13 47.5 / 38.9; mixed p = 13 104.7 / 80.0, p = 14
-// 91.2 / 82.3, p = 15 107.2 / 92.2; FP64 p = 11 about equal).
-constexpr size_t kPipeMaxSmem = 226 * 1024;
+// Largest shared-memory plan the pipelined kernel is used with: the 227 KB a
+// block may opt in to (one block plus the 1 KB per-block reservation fits the
+// SM's 228 KB).  Plans above 110 KB run one block per SM; its copy ring still
+// overlaps the next tile's loads with compute, which measured faster than the
+// one-tile-per-block kernel there (G DOF-updates/s, one-block pipelined / one
+// tile per block: FP64 p = 12 54.7 / 46.9, p = 13 47.5 / 38.9; mixed p = 13
+// 104.7 / 80.0, p = 14 91.2 / 82.3, p = 15 107.2 / 92.2; FP64 p = 11 about
+// equal; FP64 p = 14, whose plan is 231,648 bytes, stage time 0.326 / 0.368 ms).
+constexpr size_t kPipeMaxSmem = 227 * 1024;
 // Shared memory of one SM and the per-block reservation of the driver.
 constexpr size_t kSmemPerSM = 228 * 1024;
 constexpr size_t kSmemPerBlockReserved = 1024;
