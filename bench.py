@@ -1,11 +1,11 @@
 """Benchmark of the B200 SCALE-DG advection RHS (one JSON line on rank 0).
 
-Workload (default): plain FP64 DG advection at 32^3 elements, p = 7
-(16,777,216 DOF), the OPT1-equivalent kernels in FMA form ("GPU"), constant
-velocity (1, 0.5, 0.25), the seeded Gaussian + Fourier initial condition,
-dt = 0.1 h / (p+1)^2.  A bench step is one SSP-RK3 time step (three
-right-hand-side evaluations fused with their stage updates).  Metric:
-DOF-updates per second per RHS evaluation = Ne*Np*3*K / time.
+Headline workload (default): plain FP64 DG advection at 32^3 elements,
+p = 7 (16,777,216 DOF), the OPT1-equivalent kernels in FMA form ("GPU"),
+constant velocity (1, 0.5, 0.25), the seeded Gaussian + Fourier initial
+condition, dt = 0.1 h / (p+1)^2.  A bench step is one SSP-RK3 time step
+(three right-hand-side evaluations fused with their stage updates).
+Metric: DOF-updates per second per RHS evaluation = Ne*Np*3*K / time.
 
   value  device-resident state, K steps timed with CUDA events on the
          library's stream (inputs of 537 MB > 126 MB L2, so no L2 flush).
@@ -19,6 +19,22 @@ DOF-updates per second per RHS evaluation = Ne*Np*3*K / time.
          measured HBM copy bandwidth.
   cpu_baseline  the CPU oracle (restated reference OPT1 path) on the host
          cores, a bounded sample of the same workload (rank 0, N = 1).
+
+The default run also measures, in the same process and after the headline,
+the other forms under keys of their own (each with its value, stage times,
+roofline, clocks and, for the mixed form, its accuracy):
+  mixed_32c_p7, mixed_16c_p15  the mixed-precision form (FP32 state and
+         derivatives, FP64 RK accumulation), divergence-free velocity;
+  batch_fp64, batch_mixed  the 96-instance batched ensemble (Ne per axis
+         U{6..24}, p in {3,5,7,9}), CUDA-graph RK steps, autotuned tiles;
+  served  a short Poisson request stream at ~80 % load (--form-requests
+         requests; the served workload runs the long stream).
+--forms none skips them.
+
+Other workloads (--workload): fp64_8c_p3, mixed_32c_p7, mixed_16c_p15,
+batch_fp64, batch_mixed, served, divlike_var5_32c_p7 (the five-field
+derivative operator) and pscan (one instance of ~16.8 M DOF per order
+p = 1..15, FP64 and mixed, through the autotuned batch path).
 
 --impl reference runs the reference's CPU path (the oracle restatement; the
 Fortran reference cannot be compiled in this image) on all host threads, a
@@ -42,32 +58,34 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "scale-dg-kernel-extraction_b200"))
 
-WORKLOADS = {
-    # name: (NeX, NeY, NeZ, p, flags-name, vel)
-    "fp64_32c_p7": (32, 32, 32, 7, "GPU", (1.0, 0.5, 0.25)),
-    "fp64_8c_p3": (8, 8, 8, 3, "GPU", (1.0, 0.5, 0.25)),
-    "mixed_32c_p7": (32, 32, 32, 7, "MIXED", "divfree"),
-    "mixed_16c_p15": (16, 16, 16, 15, "MIXED", "divfree"),
-}
+from sdg_b200.workloads import (WORKLOADS, IC_SEED, batch_composition,  # noqa: E402
+                                dt_for, fields_kwargs, served_stream)
+
+METRIC = "DOF-updates/s per RHS eval"
+FLAGS = {"GPU": 0, "OPT1": 1, "GENERAL": 1 | 2, "MIXED": 4}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="fp64_32c_p7",
                     choices=sorted(WORKLOADS) + ["batch_fp64", "batch_mixed", "served",
-                                                 "divlike_var5_32c_p7"])
-    ap.add_argument("--requests", type=int, default=200,
+                                                 "divlike_var5_32c_p7", "pscan"])
+    ap.add_argument("--forms", default="all", choices=["all", "none"],
+                    help="headline run: also measure the mixed, batched and served forms")
+    ap.add_argument("--requests", type=int, default=2000,
                     help="served workload: number of requests in the stream")
+    ap.add_argument("--form-requests", type=int, default=40,
+                    help="the served form of the default run: requests in its stream")
     ap.add_argument("--seq-sample", type=int, default=12,
-                    help="served workload: requests solved one at a time for comparison")
+                    help="served: requests solved one at a time for comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+    ap.add_argument("--cpu-seconds", type=float, default=8.0,
                     help="budget of the CPU-baseline sample")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_env():
@@ -208,18 +226,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
-def build_problem(workload, sdg):
-    NeX, NeY, NeZ, p, kind, vel = WORKLOADS[workload]
-    flags = {"GPU": 0, "OPT1": sdg.FLAG_EXACT, "MIXED": sdg.FLAG_MIXED}[kind]
+def gpu_index(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            return int(vis.split(",")[local])
+        except (ValueError, IndexError):
+            pass
+    return local
+
+
+def workload_config(name, world):
+    """The config dict of a single-mesh workload (identical in both arms)."""
+    NeX, NeY, NeZ, p, form, vel, nstep = WORKLOADS[name]
+    return {"workload": name, "mesh": [NeX, NeY, NeZ], "p": p,
+            "dof_per_gpu": NeX * NeY * NeZ * (p + 1) ** 3, "rhs_evals_per_step": 3,
+            "dt": dt_for(max(NeX, NeY, NeZ), p),
+            "velocity": vel if vel == "divfree" else list(vel), "ic_seed": IC_SEED,
+            "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas{world}" if world > 1 else "single"}
+
+
+def build_problem(name, sdg):
+    NeX, NeY, NeZ, p, form, vel, nstep = WORKLOADS[name]
     ops = sdg.read_operators(p)
     mesh = sdg.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
-    if vel == "divfree":
-        q, u, v, w = sdg.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=1)
-    else:
-        q, u, v, w = sdg.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=0, vel=vel)
-    h = 1.0 / max(NeX, NeY, NeZ)
-    dt = 0.1 * h / (p + 1) ** 2
-    return ops, mesh, flags, (q, u, v, w), dt
+    q, u, v, w = sdg.init_fields(mesh, **fields_kwargs(vel))
+    return ops, mesh, FLAGS[form], (q, u, v, w), dt_for(max(NeX, NeY, NeZ), p)
 
 
 def stage_bytes_per_dof(mixed):
@@ -257,121 +290,34 @@ def mixed_accuracy(sdg, ops, mesh, fields, dt, nstep):
             "mass_drift_f64": float((mass_ref - mass0) / abs(mass0))}
 
 
-def cpu_baseline(workload, seconds):
-    """The CPU oracle (restated reference OPT1 path) on all host threads:
-    repeated tendency evaluations of the same workload for ~`seconds`."""
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import orc
-    NeX, NeY, NeZ, p, kind, vel = WORKLOADS[workload]
-    ops = orc.read_operators(p)
-    mesh = orc.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
-    if vel == "divfree":
-        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=1)
-    else:
-        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=0, vel=vel)
-    orc.cal_tend(orc.OPT1, q, u, v, w, ops, mesh)  # warm-up
-    n, t0 = 0, time.perf_counter()
-    while True:
-        orc.cal_tend(orc.OPT1, q, u, v, w, ops, mesh)
-        n += 1
-        el = time.perf_counter() - t0
-        if el > seconds or n >= 200:
-            break
-    dof = mesh.Ne * mesh.Np
-    return {"value": dof * n / el, "unit": "DOF-updates/s per RHS eval",
-            "cores": orc.num_threads(), "kind": "port",
-            "sample": f"{n} tendency evaluations (OPT1 order) of the {workload} "
-                      f"workload, {el:.1f} s"}
-
-
-def run_reference(args):
-    """--impl reference: the reference's CPU path (oracle restatement) on all
-    host threads, RK3 steps of the same workload; rank 0 only."""
-    rank, world, local = dist_env()
-    if rank != 0:
-        return
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import orc
-    NeX, NeY, NeZ, p, kind, vel = WORKLOADS[args.workload]
-    ops = orc.read_operators(p)
-    mesh = orc.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
-    if vel == "divfree":
-        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=1)
-    else:
-        q, u, v, w = orc.init_fields(mesh, ic_kind=1, seed=2024, vel_kind=0, vel=vel)
-    dt = 0.1 / max(NeX, NeY, NeZ) / (p + 1) ** 2
-    # Bounded sample: at most ~90 s of timed CPU work.
-    t0 = time.perf_counter()
-    orc.run_rk3(orc.OPT1, q, u, v, w, ops, mesh, dt, max(1, min(args.warmup, 3)))
-    t_step = (time.perf_counter() - t0) / max(1, min(args.warmup, 3))
-    k = max(1, min(args.steps, int(90.0 / max(t_step, 1e-6))))
-    _, times = orc.run_rk3(orc.OPT1, q, u, v, w, ops, mesh, dt, k)
-    dof = mesh.Ne * mesh.Np
-    val = dof * 3 * k / times[0]
-    line = {
-        "impl": "reference", "metric": "DOF-updates/s per RHS eval", "value": val,
-        "unit": "DOF-updates/s per RHS eval", "n_gpus": args.gpus, "steps": k,
-        "warmup": args.warmup, "ms_per_step": 1e3 * times[0] / k,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "mesh": [NeX, NeY, NeZ], "p": p,
-                   "dof": dof, "evaltype": "OPT1", "nstep_timed": k},
-        "cpu_baseline": {"value": val, "unit": "DOF-updates/s per RHS eval",
-                         "cores": orc.num_threads(), "kind": "port",
-                         "sample": f"{k} of {args.steps} requested SSP-RK3 steps of the "
-                                   f"{args.workload} workload (restated reference OPT1 "
-                                   "path; the Fortran reference cannot be compiled here)"},
-        "e2e": {"value": val, "unit": "DOF-updates/s per RHS eval",
-                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-
-
-def run_ours(args):
+def time_mesh(sdg, rep, name, steps, warmup, gidx):
+    """Device-timed RK3 steps of a single-mesh workload and the per-stage
+    kernel durations.  Returns the result dict and the live objects (handle,
+    problem) for the end-to-end legs."""
     import torch
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    rep = Replicas("nccl", "cuda")
-    import sdg_b200 as sdg
-
-    ops, mesh, flags, (q, u, v, w), dt = build_problem(args.workload, sdg)
+    ops, mesh, flags, fields, dt = build_problem(name, sdg)
     mixed = bool(flags & sdg.FLAG_MIXED)
     H = sdg.Handle(ops, mesh, flags)
-    H.set_state(q, u, v, w)
+    H.set_state(*fields)
     stream = torch.cuda.ExternalStream(H.stream())
     dof = mesh.Ne * mesh.Np
-
-    barrier = rep.barrier
-    max_over_ranks = rep.max
-
-    # ---- warm-up ----
-    H.rk3_steps(dt, args.warmup)
+    H.rk3_steps(dt, warmup)
     H.synchronize()
-
-    # ---- timed region: K RK3 steps, device-resident ----
     l0 = H.launch_count()
-    gpu_idx = local
-    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-    if vis:
-        try:
-            gpu_idx = int(vis.split(",")[local])
-        except ValueError:
-            pass
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_idx) as clk:
-        barrier()
+    with ClockSampler(gidx) as clk:
+        rep.barrier()
         ev0.record(stream)
-        H.rk3_steps(dt, args.steps)
+        H.rk3_steps(dt, steps)
         ev1.record(stream)
         H.synchronize()
-        barrier()
+        rep.barrier()
     t = ev0.elapsed_time(ev1) * 1e-3
     launches = H.launch_count() - l0
-    t_max = max_over_ranks(t)
-    value = world * dof * 3 * args.steps / t_max
-
-    # ---- per-stage kernel durations (roofline) ----
+    t_max = rep.max(t)
+    value = rep.world * dof * 3 * steps / t_max
+    # Per-stage kernel durations on the launching stream (roofline).
     reps = 30
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(reps)]
     for r in range(reps):
@@ -383,24 +329,266 @@ def run_ours(args):
     stage_ms = [statistics.median(evs[r][s - 1].elapsed_time(evs[r][s]) for r in range(reps))
                 for s in (1, 2, 3)]
     bpd = stage_bytes_per_dof(mixed)
-    alg_bytes = [b * dof for b in bpd]
-    achieved = sum(alg_bytes) / (sum(stage_ms) * 1e-3) / 1e9
+    achieved = sum(b * dof for b in bpd) / (sum(stage_ms) * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic(args.workload)
+    res = {"value": value, "unit": METRIC, "ms_per_step": 1e3 * t_max / steps,
+           "steps": steps, "warmup": warmup, "dtype": "f32+f64" if mixed else "f64",
+           "config": workload_config(name, rep.world),
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                        "traffic": profiled_traffic(name),
+                        "kernel": "tend_pipe_kernel (fused flux+volume+lift+RK stage)",
+                        "stage_ms": stage_ms, "alg_bytes_per_dof": bpd},
+           "clocks": clk.summary(), "gpu_launches": launches}
+    return res, (H, ops, mesh, flags, fields, dt)
+
+
+def cpu_baseline(workload, seconds):
+    """The CPU oracle (restated reference OPT1 path) on all host threads:
+    repeated tendency evaluations of the same workload for ~`seconds`."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import orc
+    NeX, NeY, NeZ, p, form, vel, nstep = WORKLOADS[workload]
+    ops = orc.read_operators(p)
+    mesh = orc.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
+    q, u, v, w = orc.init_fields(mesh, **fields_kwargs(vel))
+    orc.cal_tend(orc.OPT1, q, u, v, w, ops, mesh)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        orc.cal_tend(orc.OPT1, q, u, v, w, ops, mesh)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 200:
+            break
+    dof = mesh.Ne * mesh.Np
+    return {"value": dof * n / el, "unit": METRIC, "cores": orc.num_threads(), "kind": "port",
+            "sample": f"{n} tendency evaluations (OPT1 order) of the {workload} "
+                      f"workload, {el:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (oracle restatement) on all
+    host threads, RK3 steps of the same workload; rank 0 only."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    if args.workload not in WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"the reference has no {args.workload} form (one mesh per "
+                          "process, FP64 only)"}), flush=True)
+        return
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import orc
+    NeX, NeY, NeZ, p, form, vel, nstep = WORKLOADS[args.workload]
+    ops = orc.read_operators(p)
+    mesh = orc.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
+    q, u, v, w = orc.init_fields(mesh, **fields_kwargs(vel))
+    dt = dt_for(max(NeX, NeY, NeZ), p)
+    # Bounded sample: at most ~90 s of timed CPU work.
+    t0 = time.perf_counter()
+    orc.run_rk3(orc.OPT1, q, u, v, w, ops, mesh, dt, max(1, min(args.warmup, 3)))
+    t_step = (time.perf_counter() - t0) / max(1, min(args.warmup, 3))
+    k = max(1, min(args.steps, int(90.0 / max(t_step, 1e-6))))
+    _, times = orc.run_rk3(orc.OPT1, q, u, v, w, ops, mesh, dt, k)
+    dof = mesh.Ne * mesh.Np
+    val = dof * 3 * k / times[0]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": k, "warmup": args.warmup,
+        "ms_per_step": 1e3 * times[0] / k, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "evaltype": "OPT1 (CPU, OpenMP)",
+        "config": workload_config(args.workload, args.gpus),
+        "cpu_baseline": {"value": val, "unit": METRIC, "cores": orc.num_threads(),
+                         "kind": "port",
+                         "sample": f"{k} of {args.steps} requested SSP-RK3 steps of the "
+                                   f"{args.workload} workload (restated reference OPT1 "
+                                   "path; the Fortran reference cannot be compiled here)"},
+        "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Batched ensemble and served stream
+# ---------------------------------------------------------------------------
+class BatchFields:
+    """Host fields of the batched composition, generated once and shared by
+    the FP64 and mixed batches."""
+
+    def __init__(self, sdg):
+        self.comp = batch_composition()
+        self.ops = {p: sdg.read_operators(p) for p in sorted({c["p"] for c in self.comp})}
+        self.fields = []
+        for it in self.comp:
+            vel = tuple(sdg.random_velocity(it["seed"]))
+            self.fields.append(sdg.box_fields(it["ne"], it["ne"], it["ne"], it["p"],
+                                              self.ops[it["p"]].x1D, ic_kind=1,
+                                              seed=it["seed"], vel_kind=0, vel=vel))
+
+
+def time_batch(sdg, rep, mixed, steps, warmup, gidx, bf):
+    """K RK3 steps of the 96-instance ensemble (graph replays)."""
+    b = sdg.Batch(sdg.FLAG_MIXED if mixed else 0)
+    for it, f in zip(bf.comp, bf.fields):
+        b.add(it["ne"], it["ne"], it["ne"], it["p"], bf.ops[it["p"]], *f, it["dt"])
+    b.commit(autotune=True)
+    b.run(warmup)
+    info0 = b.info()
+    with ClockSampler(gidx) as clk:
+        rep.barrier()
+        b.run(steps)
+        rep.barrier()
+    info = b.info()
+    b.close()
+    t = info["run_s"] - info0["run_s"]
+    dof = info["dof"]
+    value = rep.rate(dof * 3 * steps, t)
+    t = rep.max(t)
+    bpd = stage_bytes_per_dof(mixed)
+    achieved = dof * sum(bpd) * steps / t / 1e9
+    peak, peak_kind = measured_peaks()
+    gdof = {}
+    for it in bf.comp:
+        gdof[it["p"]] = gdof.get(it["p"], 0) + it["ne"] ** 3 * (it["p"] + 1) ** 3
+    names = {1: "block", 2: "pipe", 3: "block8"}
+    groups = []
+    for g in info["groups"]:
+        ms = {"pipe": g["ms_pipe"], "block": g["ms_block"], "block8": g["ms_block8"]}
+        chosen = ms[names.get(g["variant"], "pipe")]
+        gb = gdof[g["p"]] * bpd[1] / (chosen * 1e-3) / 1e9 if chosen > 0 else None
+        groups.append({"p": g["p"], "dof": gdof[g["p"]], "tiles": g["tiles"],
+                       "variant": names.get(g["variant"], str(g["variant"])),
+                       "stage2_ms": {k: round(v, 4) for k, v in ms.items() if v > 0},
+                       "stage2_frac": gb / peak if gb else None})
+    return {"value": value, "unit": METRIC, "ms_per_step": 1e3 * t / steps, "steps": steps,
+            "warmup": warmup, "dtype": "f32+f64" if mixed else "f64",
+            "config": {"workload": "batch_mixed" if mixed else "batch_fp64",
+                       "instances": len(bf.comp), "dof_total": dof,
+                       "ne_per_axis": "U{6..24}", "p": [3, 5, 7, 9], "nstep": 100,
+                       "l2": "inputs larger than L2 (no flush)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "kernel": "tend_pipe_kernel, batched tile tables",
+                         "alg_bytes_per_dof": bpd, "groups": groups},
+            "clocks": clk.summary(),
+            "gpu_launches": 3 * len(info["groups"]) * steps}
+
+
+def time_served(sdg, rep, nreq, seq_sample, gidx):
+    """Poisson request stream at ~80 % load against the serving loop; the
+    arrival rate comes from one-at-a-time FP64 solves of the first requests."""
+    reqs, rng = served_stream(nreq)
+    ops = {p: sdg.read_operators(p) for p in range(3, 12)}
+    fields = []
+    for r in reqs:
+        vel = tuple(sdg.random_velocity(r["seed"]))
+        fields.append(sdg.box_fields(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D,
+                                     ic_kind=1, seed=r["seed"], vel_kind=0, vel=vel))
+    work = [r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"] for r in reqs]
+    n_seq = min(len(reqs), seq_sample)
+    t_seq, w_seq = 0.0, 0
+    for r, f in zip(reqs[:n_seq], fields[:n_seq]):
+        m = sdg.mesh_setup(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D)
+        h = sdg.Handle(ops[r["p"]], m, 0)
+        full = [np.zeros((m.Np, m.NeA), order="F") for _ in range(4)]
+        n = m.Np * m.Ne
+        for dst, src in zip(full, f):
+            dst.reshape(-1, order="F")[:n] = src.reshape(-1, order="F")[:n]
+        h.set_state(*full)
+        h.synchronize()
+        t0 = time.perf_counter()
+        h.rk3_steps(r["dt"], r["nstep"])
+        h.synchronize()
+        t_seq += time.perf_counter() - t0
+        w_seq += r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"]
+        h.close()
+        del m, full
+    seq_rate = w_seq / t_seq
+    lam = 0.8 * seq_rate / float(np.mean(work))   # requests per second at ~80 % load
+    gaps = rng.exponential(1.0 / lam, size=len(reqs))
+    srv = sdg.Server()
+    with ClockSampler(gidx) as clk:
+        rep.barrier()
+        t_start = time.perf_counter()
+        ids = []
+        t_next = t_start
+        for r, f, g in zip(reqs, fields, gaps):
+            t_next += g
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]], *f,
+                                  r["dt"], r["nstep"], mixed=r["mixed"]))
+        srv.wait(0)
+        makespan = time.perf_counter() - t_start
+    polls = [srv.poll(i) for i in ids]
+    tts = np.array([p[2] for p in polls])
+    qwait = np.array([p[1] for p in polls])
+    st = srv.stats()
+    srv.close()
+    total = float(sum(work))
+    value = rep.rate(total, makespan)
+    makespan = rep.max(makespan)
+    busy = rep.max(st["busy_s"])
+    busy_rate = rep.sum(st["dof_steps"] * 3) / max(busy, 1e-9)
+    bytes_step = sum(r["ne"] ** 3 * (r["p"] + 1) ** 3 * r["nstep"] *
+                     sum(stage_bytes_per_dof(r["mixed"])) for r in reqs)
+    peak, peak_kind = measured_peaks()
+    achieved = rep.sum(bytes_step) / max(busy, 1e-9) / 1e9
+    return {"value": value, "unit": METRIC, "ms_per_step": 1e3 * makespan / len(reqs),
+            "steps": len(reqs), "warmup": 0, "dtype": "f32+f64",
+            "config": {"workload": "served", "requests": len(reqs),
+                       "arrival_rate_per_s": lam, "load": 0.8, "ne_per_axis": "U{8..32}",
+                       "p": "U{3..11}", "nstep": "U{50..400}", "fp32_fraction":
+                       float(np.mean([r["mixed"] for r in reqs]))},
+            "served": {"p50_tts_s": rep.max(np.percentile(tts, 50)),
+                       "p99_tts_s": rep.max(np.percentile(tts, 99)),
+                       "mean_tts_s": float(tts.mean()),
+                       "p50_queue_s": float(np.percentile(qwait, 50)),
+                       "p99_queue_s": float(np.percentile(qwait, 99)),
+                       "makespan_s": makespan, "device_busy_s": busy,
+                       "throughput_busy": busy_rate,
+                       "one_at_a_time_fp64": rep.sum(seq_rate),
+                       "busy_vs_one_at_a_time": busy_rate / rep.sum(seq_rate),
+                       "one_at_a_time_sample": n_seq,
+                       "iterations": st["iterations"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "over": "device-busy time",
+                         "kernel": "tend_pipe_kernel, batched tile tables"},
+            "clocks": clk.summary()}
+
+
+# ---------------------------------------------------------------------------
+# Arms
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
+    import sdg_b200 as sdg
+    gidx = gpu_index(local)
+
+    head, (H, ops, mesh, flags, (q, u, v, w), dt) = time_mesh(
+        sdg, rep, args.workload, args.steps, args.warmup, gidx)
+    mixed = bool(flags & sdg.FLAG_MIXED)
+    dof = mesh.Ne * mesh.Np
 
     # ---- e2e: RK3 steps through the C ABI with host buffers ----
-    n_e2e = max(3, min(20, args.steps // 50))
+    n_e2e = max(3, min(20, args.steps // 10))
     NE = mesh.Np * mesh.Ne
     q_pin = torch.empty(NE, dtype=torch.float64, pin_memory=True)
     q_pin.numpy()[:] = q.reshape(-1, order="F")[:NE]
-    barrier()
+    rep.barrier()
     t0 = time.perf_counter()
     qp = q_pin.numpy()
     for _ in range(n_e2e):
         H.set_field(sdg.FIELD_Q, qp)
         H.rk3_steps(dt, 1)
         H.get_field(sdg.FIELD_Q, out=qp)
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    t_e2e = rep.max(time.perf_counter() - t0)
     e2e = world * dof * 3 * n_e2e / t_e2e
 
     # ---- e2e of the drop-in tendency call (FP64 handles only) ----
@@ -414,70 +602,76 @@ def run_ours(args):
         arrs = [pt.numpy().reshape(mesh.Np, mesh.NeA, order="F") for pt in pins]
         Hc.cal_tend(*arrs[:4], dqdt=arrs[4])
         n_ct = 5
-        barrier()
+        rep.barrier()
         t0 = time.perf_counter()
         for _ in range(n_ct):
             Hc.cal_tend(*arrs[:4], dqdt=arrs[4])
-        t_ct = max_over_ranks(time.perf_counter() - t0)
-        e2e_ct = {"value": world * dof * n_ct / t_ct, "unit": "DOF-updates/s per RHS eval",
+        t_ct = rep.max(time.perf_counter() - t0)
+        e2e_ct = {"value": world * dof * n_ct / t_ct, "unit": METRIC,
                   "h2d_bytes_per_step": 4 * NA * 8, "d2h_bytes_per_step": NE * 8}
         Hc.close()
+        del pins, arrs
+    H.close()
+    del q_pin
 
-    # ---- accuracy of the mixed form against FP64 after nstep steps ----
     accuracy = None
     if mixed:
         accuracy = mixed_accuracy(sdg, ops, mesh, (q, u, v, w), dt, 200)
+    del q, u, v, w, mesh
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, args.cpu_seconds)
 
+    # ---- the other forms, same process (default run) ----
+    forms = {}
+    if args.forms == "all" and args.workload == "fp64_32c_p7":
+        for name in ("mixed_32c_p7", "mixed_16c_p15"):
+            r, (Hm, o, m, fl, fd, dtm) = time_mesh(sdg, rep, name, args.steps, args.warmup,
+                                                   gidx)
+            Hm.close()
+            r["accuracy"] = mixed_accuracy(sdg, o, m, fd, dtm, WORKLOADS[name][6])
+            r["vs_fp64_32c_p7"] = r["value"] / head["value"]
+            forms[name] = r
+            del Hm, o, m, fd
+        bf = BatchFields(sdg)
+        for mx in (False, True):
+            forms["batch_mixed" if mx else "batch_fp64"] = time_batch(
+                sdg, rep, mx, max(3, min(args.steps, 20)), max(3, args.warmup), gidx, bf)
+        forms["batch_fp64"]["vs_fp64_32c_p7"] = forms["batch_fp64"]["value"] / head["value"]
+        forms["batch_mixed"]["vs_fp64_32c_p7"] = forms["batch_mixed"]["value"] / head["value"]
+        del bf
+        forms["served"] = time_served(sdg, rep, args.form_requests,
+                                      min(args.seq_sample, 6), gidx)
+
     if rank == 0:
-        NeX, NeY, NeZ, p, kind, vel = WORKLOADS[args.workload]
         line = {
-            "metric": "DOF-updates/s per RHS eval", "value": value,
-            "unit": "DOF-updates/s per RHS eval", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "metric": METRIC, "value": head["value"], "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "mesh": [NeX, NeY, NeZ], "p": p,
-                       "dof_per_gpu": dof, "evaltype": kind,
-                       "rhs_evals_per_step": 3, "dt": dt,
-                       "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"replicas{world}" if world > 1 else "single"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": f"{peak_kind} hbm_gbs",
-                         "traffic": traffic,
-                         "kernel": "tend_pipe_kernel (fused flux+volume+lift+RK stage)",
-                         "stage_ms": stage_ms,
-                         "alg_bytes_per_dof": bpd},
-            "e2e": {"value": e2e, "unit": "DOF-updates/s per RHS eval",
+            "dtype": head["dtype"], "data": "synthetic",
+            "evaltype": {0: "GPU (fast FP64)", 1: "OPT1 (bit-exact)", 3: "GENERAL (bit-exact)",
+                         4: "MIXED"}.get(flags, str(flags)),
+            "config": head["config"],
+            "roofline": head["roofline"],
+            "e2e": {"value": e2e, "unit": METRIC,
                     "h2d_bytes_per_step": NE * 8, "d2h_bytes_per_step": NE * 8,
                     "api": "sdg_set_field + sdg_rk3_steps + sdg_get_field per step"},
             "e2e_cal_tend": e2e_ct,
             "accuracy": accuracy,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
-            "gpu_launches": launches,
+            "clocks": head["clocks"],
+            "gpu_launches": head["gpu_launches"],
         }
+        line.update(forms)
         print(json.dumps(line), flush=True)
-    H.close()
     rep.close()
 
 
-def ensemble_instances(n, seed, ne_range, p_choices, rng_nstep=None):
-    """Seeded instance list: cubic boxes Ne ~ U{ne_range}, p from p_choices,
-    constant velocity U[-1,1]^3, dt = 0.1 h / (p+1)^2."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for k in range(n):
-        ne = int(rng.integers(ne_range[0], ne_range[1] + 1))
-        p = int(rng.choice(p_choices))
-        nstep = int(rng.integers(rng_nstep[0], rng_nstep[1] + 1)) if rng_nstep else None
-        out.append({"ne": ne, "p": p, "seed": 1000 + k, "nstep": nstep,
-                    "dt": 0.1 / ne / (p + 1) ** 2})
-    return out
+def run_mesh_only(args):
+    """A single-mesh workload other than the headline, without the forms."""
+    args.forms = "none"
+    run_ours(args)
 
 
 def run_batch(args):
@@ -489,44 +683,88 @@ def run_batch(args):
     rep = Replicas("nccl", "cuda")
     import sdg_b200 as sdg
     mixed = args.workload == "batch_mixed"
-    inst = ensemble_instances(96, 4, (6, 24), [3, 5, 7, 9])
-    b = sdg.Batch(sdg.FLAG_MIXED if mixed else 0)
-    ops = {p: sdg.read_operators(p) for p in (3, 5, 7, 9)}
-    for it in inst:
-        vel = tuple(sdg.random_velocity(it["seed"]))
-        f = sdg.box_fields(it["ne"], it["ne"], it["ne"], it["p"], ops[it["p"]].x1D,
-                           ic_kind=1, seed=it["seed"], vel_kind=0, vel=vel)
-        b.add(it["ne"], it["ne"], it["ne"], it["p"], ops[it["p"]], *f, it["dt"])
-    b.commit(autotune=True)
-    b.run(args.warmup)
-    info0 = b.info()
-    with ClockSampler(local) as clk:
-        rep.barrier()
-        b.run(args.steps)
-        rep.barrier()
-    info = b.info()
-    t = info["run_s"] - info0["run_s"]
-    dof = info["dof"]
-    value = rep.rate(dof * 3 * args.steps, t)
-    t = rep.max(t)
-    groups = [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in g.items()}
-              for g in info["groups"]]
-    b.close()
+    r = time_batch(sdg, rep, mixed, args.steps, args.warmup, gpu_index(local), BatchFields(sdg))
     torch.cuda.synchronize()
     rep.close()
     if rank != 0:
         return
-    line = {"metric": "DOF-updates/s per RHS eval", "value": value,
-            "unit": "DOF-updates/s per RHS eval", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "instances": len(inst), "dof_total": dof,
-                       "ne_per_axis": "U{6..24}", "p": [3, 5, 7, 9],
-                       "groups": groups,
-                       "parallelism": f"replicas{world}" if world > 1 else "single"},
-            "clocks": clk.summary()}
+    r["config"]["parallelism"] = f"replicas{world}" if world > 1 else "single"
+    line = {"metric": METRIC, "n_gpus": world, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic"}
+    line.update(r)
     print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    """Served request stream: Poisson arrivals at ~80% load; Ne/axis
+    U{8..32}, p U{3..11}, nstep U{50..400}, FP32/FP64 flag.  A one-at-a-time
+    FP64 run of the first requests gives the comparison throughput.  With N
+    ranks each GPU serves its own copy of the stream; the aggregate is all
+    ranks' work over the slowest makespan and the percentiles are the worst
+    rank's."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
+    import sdg_b200 as sdg
+    r = time_served(sdg, rep, args.requests, args.seq_sample, gpu_index(local))
+    rep.close()
+    if rank != 0:
+        return
+    r["config"]["parallelism"] = f"replicas{world}" if world > 1 else "single"
+    line = {"metric": METRIC, "n_gpus": world, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic"}
+    line.update(r)
+    print(json.dumps(line), flush=True)
+
+
+def run_pscan(args):
+    """Per-order map: for p = 1..15, one periodic box of ~16.8 M DOF, FP64 and
+    mixed, autotuned through the batch path; K RK3 steps each.  frac uses the
+    mean algorithmic bytes per stage (45.3 B/DOF FP64, 28 B/DOF mixed)."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
+    import sdg_b200 as sdg
+    peak, peak_kind = measured_peaks()
+    names = {1: "Block", 2: "Pipe", 3: "BlockOcc"}
+    rows = []
+    for mixed in (False, True):
+        for p in range(1, 16):
+            nq = p + 1
+            N = max(2, round((16.8e6 / nq ** 3) ** (1 / 3)))
+            ops = sdg.read_operators(p)
+            f = sdg.box_fields(N, N, N, p, ops.x1D, ic_kind=1, seed=7, vel_kind=0,
+                               vel=(1.0, 0.5, 0.25))
+            b = sdg.Batch(sdg.FLAG_MIXED if mixed else 0)
+            b.add(N, N, N, p, ops, *f, dt_for(N, p))
+            del f
+            b.commit(autotune=True)
+            b.run(max(3, args.warmup))
+            i0 = b.info()
+            b.run(args.steps)
+            i1 = b.info()
+            b.close()
+            t = rep.max(i1["run_s"] - i0["run_s"])
+            dof = i1["dof"]
+            g = i1["groups"][0]
+            bpd = sum(stage_bytes_per_dof(mixed)) / 3
+            G = world * dof * 3 * args.steps / t
+            rows.append({"p": p, "mixed": mixed, "mesh": N, "dof": dof,
+                         "G_dof_updates_per_s": G / 1e9, "frac": G * bpd / 1e9 / peak,
+                         "variant": names.get(g["variant"], g["variant"]),
+                         "stage2_ms": {"pipe": g["ms_pipe"], "block": g["ms_block"],
+                                       "block8": g["ms_block8"]}})
+    rep.close()
+    if rank != 0:
+        return
+    print(json.dumps({"metric": f"{METRIC} per order", "unit": METRIC, "n_gpus": world,
+                      "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                      "data": "synthetic", "peak": peak, "peak_source": f"{peak_kind} hbm_gbs",
+                      "config": {"workload": "pscan", "dof_per_order": "~16.8 M",
+                                 "velocity": [1.0, 0.5, 0.25]},
+                      "per_order": rows}), flush=True)
 
 
 def run_derivative(args):
@@ -560,16 +798,9 @@ def run_derivative(args):
     for _ in range(args.warmup):
         call()
     torch.cuda.synchronize()
-    gpu_idx = local
-    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
-    if vis:
-        try:
-            gpu_idx = int(vis.split(",")[local])
-        except ValueError:
-            pass
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_idx) as clk:
+    with ClockSampler(gpu_index(local)) as clk:
         rep.barrier()
         ev0.record(stream)
         for _ in range(args.steps):
@@ -647,89 +878,6 @@ def run_derivative(args):
     print(json.dumps(line), flush=True)
 
 
-def run_served(args):
-    """Served request stream: Poisson arrivals at ~80% load; Ne/axis
-    U{8..32}, p U{3..11}, nstep U{50..400}, FP32/FP64 flag.  The stream is
-    shortened to --requests requests (the full 2,000 take ~3 minutes of GPU
-    time at this load); a one-at-a-time FP64 run of the first requests gives
-    the comparison throughput.  With N ranks each GPU serves its own copy of
-    the stream; the aggregate is all ranks' work over the slowest makespan
-    and the percentiles are the worst rank's."""
-    import torch
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    rep = Replicas("nccl", "cuda")
-    import sdg_b200 as sdg
-    reqs = ensemble_instances(args.requests, 5, (8, 32), list(range(3, 12)), (50, 400))
-    rng = np.random.default_rng(6)
-    for r in reqs:
-        r["mixed"] = bool(rng.integers(0, 2))
-    ops = {p: sdg.read_operators(p) for p in range(3, 12)}
-    fields = []
-    for r in reqs:
-        vel = tuple(sdg.random_velocity(r["seed"]))
-        fields.append(sdg.box_fields(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D,
-                                     ic_kind=1, seed=r["seed"], vel_kind=0, vel=vel))
-    work = [r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"] for r in reqs]
-    # Service-rate estimate from the one-at-a-time FP64 solves of a sample.
-    n_seq = min(len(reqs), args.seq_sample)
-    t_seq, w_seq = 0.0, 0
-    for r, f in zip(reqs[:n_seq], fields[:n_seq]):
-        m = sdg.mesh_setup(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D)
-        h = sdg.Handle(ops[r["p"]], m, 0)
-        h.set_state(*f)
-        h.synchronize()
-        t0 = time.perf_counter()
-        h.rk3_steps(r["dt"], r["nstep"])
-        h.synchronize()
-        t_seq += time.perf_counter() - t0
-        w_seq += r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"]
-        h.close()
-        del m
-    seq_rate = w_seq / t_seq
-    mean_work = float(np.mean(work))
-    lam = 0.8 * seq_rate / mean_work           # requests per second at ~80% load
-    gaps = rng.exponential(1.0 / lam, size=len(reqs))
-    srv = sdg.Server()
-    rep.barrier()
-    t_start = time.perf_counter()
-    ids = []
-    for r, f, g in zip(reqs, fields, gaps):
-        time.sleep(g)
-        ids.append(srv.submit(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]], *f,
-                              r["dt"], r["nstep"], mixed=r["mixed"]))
-    srv.wait(0)
-    makespan = time.perf_counter() - t_start
-    tts = np.array([srv.poll(i)[2] for i in ids])
-    st = srv.stats()
-    srv.close()
-    total = float(sum(work))
-    value = rep.rate(total, makespan)
-    makespan = rep.max(makespan)
-    p50 = rep.max(np.percentile(tts, 50))
-    p99 = rep.max(np.percentile(tts, 99))
-    busy = rep.max(st["busy_s"])
-    busy_rate = rep.sum(st["dof_steps"] * 3) / max(busy, 1e-9)
-    seq_rate = rep.sum(seq_rate)
-    rep.close()
-    if rank != 0:
-        return
-    line = {"metric": "DOF-updates/s per RHS eval", "value": value,
-            "unit": "DOF-updates/s per RHS eval", "n_gpus": world, "steps": len(reqs),
-            "warmup": 0, "ms_per_step": 1e3 * makespan / len(reqs),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": "served", "requests": len(reqs),
-                       "arrival_rate_per_s": lam, "load": 0.8,
-                       "ne_per_axis": "U{8..32}", "p": "U{3..11}", "nstep": "U{50..400}",
-                       "parallelism": f"replicas{world}" if world > 1 else "single"},
-            "served": {"p50_tts_s": p50, "p99_tts_s": p99,
-                       "mean_tts_s": float(tts.mean()), "makespan_s": makespan,
-                       "device_busy_s": busy, "throughput_busy": busy_rate,
-                       "one_at_a_time_fp64": seq_rate, "one_at_a_time_sample": n_seq}}
-    print(json.dumps(line), flush=True)
-
-
 def main():
     args = parse()
     if args.impl == "reference":
@@ -740,6 +888,10 @@ def main():
         run_served(args)
     elif args.workload == "divlike_var5_32c_p7":
         run_derivative(args)
+    elif args.workload == "pscan":
+        run_pscan(args)
+    elif args.workload != "fp64_32c_p7":
+        run_mesh_only(args)
     else:
         run_ours(args)
 

@@ -204,6 +204,18 @@ long long sdg_launch_count(sdg_handle* h);
  * compute identical results; the choice only affects speed. */
 int sdg_set_kernel_variant(sdg_handle* h, int variant);
 
+/* Test hook for the failure path of the bounded waits (no reference
+ * counterpart: the reference has no device waits; its only error handling
+ * is the file-open check of main.f90:117-122).  With tile >= 0, the
+ * persistent bulk-copy kernel of this handle never issues the copies of
+ * element tile `tile`, so the wait for them runs out after `spins` polls
+ * (0: the default limit); the kernel then records a timeout in the
+ * handle's status word and returns, and the next synchronising call
+ * (sdg_synchronize, sdg_get_field, sdg_minmax) fails with SDG_ERR_CUDA and
+ * clears the word.  tile < 0 restores normal operation; the handle stays
+ * usable throughout.  Only the pipelined kernel variant has waits. */
+int sdg_debug_inject_wait_timeout(sdg_handle* h, int tile, int spins);
+
 /* ---------------------------------------------------------------------
  * Batched ensembles: many independent periodic-box instances of uneven
  * size and order advanced together (the reference runs one mesh per
@@ -245,6 +257,11 @@ int sdg_batch_get(sdg_batch* b, int id, double* q);
  * stage times (ms) of the pipelined, block and 8-blocks-per-SM variants.
  * Returns the number of values available. */
 int sdg_batch_info(sdg_batch* b, double* out, int n);
+
+/* The batch's form of sdg_debug_inject_wait_timeout: tile `tile` of every
+ * group's tile table is skipped; sdg_batch_run then fails with
+ * SDG_ERR_CUDA.  A committed batch re-captures its step graph. */
+int sdg_batch_debug_inject_wait_timeout(sdg_batch* b, int tile, int spins);
 
 int sdg_batch_destroy(sdg_batch* b);
 

@@ -168,6 +168,8 @@ struct Ensemble {
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
   int* status = nullptr;
+  unsigned wait_spins = 0;  // bounded-wait spin limit (0: default)
+  int inject_skip = 0;      // test hook: tile + 1 left without copies
   std::map<int, std::unique_ptr<Ops>> ops;              // by nq
   std::map<std::pair<int, bool>, std::unique_ptr<Group>> groups;
 
@@ -422,6 +424,8 @@ struct Ensemble {
     l.stream = s;
     l.variant = g->variant;
     l.status = status;
+    l.wait_spins = wait_spins;
+    l.inject_skip = inject_skip;
     l.num_sms = num_sms;
     const double ra[3] = {0.0, 0.75, 1.0 / 3.0};
     const double rb[3] = {1.0, 0.25, 2.0 / 3.0};
@@ -605,6 +609,31 @@ struct sdg_batch {
   long long dof_steps = 0;
 };
 
+namespace {
+
+// Captures one RK step of every group, forked over the groups' streams and
+// joined back, as the batch's step graph (replayed per step).
+int capture_step(sdg_batch* b) {
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  cudaGraph_t g;
+  ENS_CUDA(cudaStreamBeginCapture(b->ens.stream, cudaStreamCaptureModeThreadLocal));
+  int rc = b->ens.step(b->ens.stream);
+  cudaError_t ee = cudaStreamEndCapture(b->ens.stream, &g);
+  if (rc) return rc;
+  if (ee != cudaSuccess)
+    return fail(SDG_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(ee));
+  ee = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ee != cudaSuccess)
+    return fail(SDG_ERR_CUDA, "batch graph instantiate failed: %s", cudaGetErrorString(ee));
+  return SDG_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int sdg_batch_create(sdg_batch** out, int flags) {
@@ -653,19 +682,7 @@ int sdg_batch_commit(sdg_batch* b, int autotune) {
   int rc;
   if (autotune && (rc = b->ens.autotune(5))) return rc;
   if ((rc = b->ens.prime())) return rc;
-  // One RK step of every group, forked over the groups' streams and joined
-  // back, captured once and replayed per step.
-  cudaGraph_t g;
-  ENS_CUDA(cudaStreamBeginCapture(b->ens.stream, cudaStreamCaptureModeThreadLocal));
-  rc = b->ens.step(b->ens.stream);
-  cudaError_t ee = cudaStreamEndCapture(b->ens.stream, &g);
-  if (rc) return rc;
-  if (ee != cudaSuccess)
-    return fail(SDG_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(ee));
-  ee = cudaGraphInstantiate(&b->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (ee != cudaSuccess)
-    return fail(SDG_ERR_CUDA, "batch graph instantiate failed: %s", cudaGetErrorString(ee));
+  if ((rc = capture_step(b))) return rc;
   ENS_CUDA(cudaEventCreate(&b->ev0));
   ENS_CUDA(cudaEventCreate(&b->ev1));
   b->committed = true;
@@ -728,6 +745,16 @@ int sdg_batch_info(sdg_batch* b, double* out, int n) {
   return static_cast<int>(v.size());
 }
 
+int sdg_batch_debug_inject_wait_timeout(sdg_batch* b, int tile, int spins) {
+  if (!b) return fail(SDG_ERR_ARG, "null batch");
+  if (spins < 0) return fail(SDG_ERR_ARG, "spins must be >= 0");
+  cudaSetDevice(b->ens.dev);
+  ENS_CUDA(cudaStreamSynchronize(b->ens.stream));
+  b->ens.inject_skip = tile >= 0 ? tile + 1 : 0;
+  b->ens.wait_spins = static_cast<unsigned>(spins);
+  return b->committed ? capture_step(b) : SDG_OK;
+}
+
 int sdg_batch_destroy(sdg_batch* b) {
   if (!b) return fail(SDG_ERR_ARG, "null batch");
   cudaSetDevice(b->ens.dev);
@@ -753,6 +780,12 @@ int sdg_batch_destroy(sdg_batch* b) {
 // done (result copied to the host, memory returned to the pool).  Requests
 // that arrive while others run join at the next step boundary, so their
 // work overlaps the others' on the device.
+// Operators submitted with a request, kept until its admission (ops_for
+// needs the arrays).
+struct PendingOps {
+  std::vector<double> D, L;
+};
+
 struct sdg_server {
   Ensemble ens;
   size_t cap = 0;
@@ -763,6 +796,8 @@ struct sdg_server {
   std::deque<Inst*> queue;
   std::vector<Inst*> active;
   std::map<int, std::unique_ptr<Inst>> all;
+  // Operators of queued requests, by request (guarded by mu, like queue).
+  std::map<const Inst*, PendingOps> pending_ops;
   int next_id = 0;
   bool stop = false;
   int error = SDG_OK;
@@ -796,17 +831,6 @@ struct sdg_server {
   bool step_once(std::vector<Inst*>& admit);
 };
 
-namespace {
-
-// Operators submitted with a request are stored in the request until
-// admission (ops_for needs the arrays); kept next to the instance.
-struct PendingOps {
-  std::vector<double> D, L;
-};
-std::map<const Inst*, PendingOps> g_pending_ops;
-
-}  // namespace
-
 bool sdg_server::step_once(std::vector<Inst*>& admit) {
   // Admission: allocate, upload, join the order's group.
   for (Inst* I : admit) {
@@ -816,8 +840,8 @@ bool sdg_server::step_once(std::vector<Inst*>& admit) {
     PendingOps po;
     {
       std::lock_guard<std::mutex> lk(mu);
-      po = std::move(g_pending_ops[I]);
-      g_pending_ops.erase(I);
+      po = std::move(pending_ops[I]);
+      pending_ops.erase(I);
     }
     rc = ens.ops_for(I->p, po.D.data(), po.L.data(), &o);
     if (!rc) rc = ens.group_for(I->nq, I->mixed, o, &g);
@@ -934,7 +958,7 @@ int sdg_serve_submit(sdg_server* s, int NeX, int NeY, int NeZ, int p, const doub
   I->id = s->next_id++;
   I->t_submit = now_s();
   I->state = kQueued;
-  g_pending_ops[I.get()] = std::move(po);
+  s->pending_ops[I.get()] = std::move(po);
   s->queue.push_back(I.get());
   *id = I->id;
   s->all[I->id] = std::move(I);
@@ -1005,10 +1029,6 @@ int sdg_serve_destroy(sdg_server* s) {
   cudaSetDevice(s->ens.dev);
   for (Inst* I : s->active) s->ens.release(I, s->ens.stream);
   cudaStreamSynchronize(s->ens.stream);
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    for (auto& kv : s->all) g_pending_ops.erase(kv.second.get());
-  }
   delete s;
   return SDG_OK;
 }

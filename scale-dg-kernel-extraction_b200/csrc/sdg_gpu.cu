@@ -187,6 +187,8 @@ struct sdg_handle {
   int variant = kVariantAuto;  // KernelVariant of the fused kernel
   int num_sms = 148;
   int* status = nullptr;       // device status word of bounded waits
+  unsigned wait_spins = 0;     // bounded-wait spin limit (0: default)
+  int inject_skip = 0;         // test hook: tile + 1 left without copies
   bool primed = false;
   cudaStream_t stream = nullptr;
   std::vector<double> D;  // row-major D(i,l)
@@ -274,6 +276,8 @@ LaunchSpec base_spec(const sdg_handle* h, bool f32) {
   s.stream = h->stream;
   s.variant = h->variant;
   s.status = h->status;
+  s.wait_spins = h->wait_spins;
+  s.inject_skip = h->inject_skip;
   s.num_sms = h->num_sms;
   return s;
 }
@@ -868,6 +872,20 @@ int sdg_set_kernel_variant(sdg_handle* h, int variant) {
   }
   h->variant = variant;
   h->primed = false;
+  return SDG_OK;
+}
+
+int sdg_debug_inject_wait_timeout(sdg_handle* h, int tile, int spins) {
+  if (!h) return fail(SDG_ERR_ARG, "null handle");
+  if (spins < 0) return fail(SDG_ERR_ARG, "spins must be >= 0");
+  cudaSetDevice(h->dev);
+  cudaStreamSynchronize(h->stream);
+  if (h->graph) {  // the step graph holds the old kernel arguments
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->inject_skip = tile >= 0 ? tile + 1 : 0;
+  h->wait_spins = static_cast<unsigned>(spins);
   return SDG_OK;
 }
 

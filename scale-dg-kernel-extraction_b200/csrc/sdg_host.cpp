@@ -10,11 +10,13 @@
 // Built with -ffp-contract=off: node coordinates and initial fields round
 // exactly like the reference's x86-64 build.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "sdg_gpu.h"
@@ -307,7 +309,10 @@ int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
   }
   const long NE = static_cast<long>(Np) * Ne;
   const double two_s2 = 2.0 * 0.1 * 0.1;  // 2 sigma^2, sigma = 0.1
-  for (long x = 0; x < NE; ++x) {
+  // Every node is independent: split the nodes over host threads (the
+  // values do not depend on the split).
+  auto fill = [&](long x0, long x1) {
+  for (long x = x0; x < x1; ++x) {
     const double px = pos_en[x], py = pos_en[x + NE], pz = pos_en[x + 2 * NE];
     if (ic_kind == 0) {
       q[x] = std::sin(two_pi * px) * std::sin(two_pi * py) * std::sin(two_pi * pz);
@@ -328,6 +333,17 @@ int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
       v[x] = std::sin(two_pi * pz);
       w[x] = std::sin(two_pi * px);
     }
+  }
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const long nthr = std::max(1L, std::min({static_cast<long>(hw ? hw : 1), 32L, NE / 65536}));
+  if (nthr == 1) {
+    fill(0, NE);
+  } else {
+    std::vector<std::thread> pool;
+    for (long t = 0; t < nthr; ++t)
+      pool.emplace_back(fill, NE * t / nthr, NE * (t + 1) / nthr);
+    for (auto& th : pool) th.join();
   }
   return SDG_OK;
 }

@@ -24,6 +24,23 @@ inline int setup_device() {
   return d;
 }
 
+// Largest dynamic shared memory a block of the current device may opt in to
+// (cudaDevAttrMaxSharedMemoryPerBlockOptin), read once per device; 0 when it
+// cannot be read.  A kernel plan above it falls back to a smaller kernel.
+inline size_t device_smem_optin() {
+  static DeviceSetup cache;
+  const int d = setup_device();
+  if (d < 0) return 0;
+  int v = cache.slot[d].load(std::memory_order_relaxed);
+  if (v == 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, d) != cudaSuccess ||
+        v <= 0)
+      return 0;
+    cache.slot[d].store(v, std::memory_order_relaxed);
+  }
+  return static_cast<size_t>(v);
+}
+
 // Summation order of the contractions for NQ > 8: OPT1's three partial sums
 // (mod_dg_optr_kernel_opt1.F90.erb:242-274) or GENERAL's sequential loop
 // (mod_dg_optr_kernel.f90:221-257).  Identical for NQ <= 8.
@@ -65,6 +82,8 @@ struct LaunchSpec {
   cudaStream_t stream;
   int variant;         // KernelVariant
   int* status;         // device status word (bounded-wait timeouts)
+  unsigned wait_spins; // spin limit of a bounded wait; 0: the default
+  int inject_skip;     // test hook: tile + 1 whose copies are skipped; 0: none
   int num_sms;         // multiprocessors of the device
   // Batched launch (pipelined kernel only): device arrays of BatchInst and
   // BatchTile (sdg_tend.cuh) and the tile count; null for one instance.

@@ -241,10 +241,15 @@ int main(int argc, char** argv) {
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   double tm[4];
   sdg_timers(h, tm);
+  // The four labels of main.f90:175-177 and mod_advect3d_eq.f90:34-35.  The
+  // boundary flux and the volume derivative + lift run fused in one kernel
+  // together with the RK stage update, so the whole kernel time is reported
+  // under the second label and the first reads 0.
   std::printf("= Report of execution time [sec]\n");
   std::printf("%30s%24.5E\n", "Main:", t_main);
   std::printf("%30s%24.5E\n", "Cal_tend:", tm[1]);
-  std::printf("%30s%24.5E\n", "Fused flux+dqdt+RK stage:", tm[1]);
+  std::printf("%30s%24.5E\n", "Element boundary flux:", 0.0);
+  std::printf("%30s%24.5E\n", "Volume derivate + surface lift:", tm[1]);
   sdg_finalize(h);
   return 0;
 }

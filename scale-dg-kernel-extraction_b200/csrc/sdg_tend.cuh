@@ -294,6 +294,11 @@ struct TendArgs {
   int nelem;            // elements in this launch
   double rk_a, rk_b, dt;
   int* status;          // device status word: nonzero after a timed-out wait
+  // Spin limit of each bounded wait of the pipelined kernel (try_wait
+  // polls), and a test hook: when inject_skip = T + 1, tile T's bulk copies
+  // are never issued, so the wait for them runs out (0: none).
+  unsigned wait_spins;
+  int inject_skip;
   // One-tile-per-block kernel: block b prefetches into L2 the inputs of
   // block b + prefetch_dist (about one resident wave ahead); 0 disables.
   int prefetch_dist;

@@ -70,6 +70,8 @@ int run(const LaunchSpec& s) {
   a.rk_b = s.rk_b;
   a.dt = s.dt;
   a.status = s.status;
+  a.wait_spins = s.wait_spins ? s.wait_spins : kWaitSpins;
+  a.inject_skip = s.inject_skip;
   a.prefetch_dist = 0;
   a.insts = static_cast<const BatchInst*>(s.batch_insts);
   a.tiles = static_cast<const BatchTile*>(s.batch_tiles);
@@ -84,7 +86,8 @@ int run(const LaunchSpec& s) {
   // Batched arrays are allocated 256-byte aligned by the batch itself.  The
   // fast pipelined kernels need the factored lift; with a verbatim table a
   // fast launch takes the one-tile-per-block kernel.
-  const bool can_pipe = P::BYTES <= kPipeMaxSmem && (EXACT || s.lift_z != nullptr) &&
+  const bool can_pipe = P::BYTES <= kPipeMaxSmem && P::BYTES <= device_smem_optin() &&
+                        (EXACT || s.lift_z != nullptr) &&
                         (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
                                    aligned(s.w) && aligned(s.escale) && aligned(s.fscale)));
   if (batch && !can_pipe) return static_cast<int>(cudaErrorNotSupported);
@@ -155,9 +158,12 @@ int run(const LaunchSpec& s) {
 #define SDG_CAT2(a, b) a##b
 #define SDG_CAT(a, b) SDG_CAT2(a, b)
 
+// Whether the plan fits both the build's limit and the current device's
+// per-block opt-in.
 template <typename TQ, typename TV, typename TC, bool STAGE>
-constexpr bool pipe_fits() {
-  return PipePlan<NQ, TQ, TV, TC, STAGE>::BYTES <= kPipeMaxSmem;
+bool pipe_fits() {
+  constexpr size_t bytes = PipePlan<NQ, TQ, TV, TC, STAGE>::BYTES;
+  return bytes <= kPipeMaxSmem && bytes <= device_smem_optin();
 }
 
 // Pipelined-kernel facts for this order: elements per tile, and whether the

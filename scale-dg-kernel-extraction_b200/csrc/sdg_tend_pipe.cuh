@@ -46,6 +46,7 @@
 namespace sdg {
 
 constexpr int kStatusWaitTimeout = 1;
+// Default spin limit of a bounded wait (polls of mbarrier.try_wait).
 constexpr unsigned kWaitSpins = 1u << 22;
 // Largest shared-memory plan the pipelined kernel is used with: the 227 KB a
 // block may opt in to (one block plus the 1 KB per-block reservation fits the
@@ -87,9 +88,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase of `bar` with the given parity.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (unsigned it = 0; it < kWaitSpins; ++it)
+// Bounded wait for the phase of `bar` with the given parity: at most
+// `spins` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  unsigned spins) {
+  for (unsigned it = 0; it < spins; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -526,6 +529,9 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
 
   // Producer: one thread fills ring slot `slot` with tile `tile`.
   auto issue = [&](int tile, int slot) {
+    // Test hook (host-set): leave this tile's slot empty, so that its wait
+    // runs out and the timeout path below is taken.
+    if (tile + 1 == A.inject_skip) return;
     const Ctx c = tile_ctx<EPB, BATCH>(A, tile, ntiles);
     unsigned char* base = slots + slot * P::SLOT;
     const void* src[6] = {c.q, c.u, c.v, c.w, c.escale, c.fscale};
@@ -590,7 +596,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     for (int f = 0; f < 6; ++f) pbc[f] = active ? ldro(C.pbase + 6 * static_cast<long>(e) + f) : 0;
 
     // ---- Wait for the tile's slot (bounded, block-uniform) -----------------
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity));
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity, A.wait_spins));
     if (!ok) {
       if (threadIdx.x == 0) {
         atomicExch(A.status, kStatusWaitTimeout);
@@ -601,7 +607,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           const int T = it + k;
           const int tk = blockIdx.x + T * gridDim.x;
           if (tk < ntiles && (T < NS || T - NS + 1 <= it - 1))
-            mbar_wait_bounded(&bars[T % NS], (T / NS) & 1);
+            mbar_wait_bounded(&bars[T % NS], (T / NS) & 1, A.wait_spins);
         }
       }
       return;

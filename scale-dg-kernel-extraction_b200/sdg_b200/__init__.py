@@ -77,6 +77,7 @@ SIGNATURES = {
     "sdg_timers": (_I, [_P, _P]),
     "sdg_launch_count": (_LL, [_P]),
     "sdg_set_kernel_variant": (_I, [_P, _I]),
+    "sdg_debug_inject_wait_timeout": (_I, [_P, _I, _I]),
     "sdg_minmax_dev_noalloc": (_I, [_P, _LL, _P, _P]),
     "sdg_divlike_dev": (_I, [_I, _I, _LL, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "sdg_gradlike_dev": (_I, [_I, _LL, _P, _P, _P, _P, _P, _I, _P]),
@@ -88,6 +89,7 @@ SIGNATURES = {
     "sdg_batch_get": (_I, [_P, _I, _P]),
     "sdg_batch_info": (_I, [_P, _P, _I]),
     "sdg_batch_destroy": (_I, [_P]),
+    "sdg_batch_debug_inject_wait_timeout": (_I, [_P, _I, _I]),
     "sdg_serve_create": (_I, [ctypes.POINTER(_P), _D]),
     "sdg_serve_submit": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _D, _I, _I,
                               ctypes.POINTER(_I)]),
@@ -367,6 +369,12 @@ class Handle:
         """0 automatic, 1 one tile per block, 2 persistent bulk-copy ring."""
         _check(lib().sdg_set_kernel_variant(self._h, variant))
 
+    def inject_wait_timeout(self, tile, spins=0):
+        """Test hook: the pipelined kernel skips the copies of element tile
+        `tile`, so its bounded wait runs out after `spins` polls and the next
+        synchronising call raises; tile < 0 turns it off."""
+        _check(lib().sdg_debug_inject_wait_timeout(self._h, tile, spins))
+
 
 # ---------------------------------------------------------------------------
 # The reference's operator/driver surface
@@ -500,6 +508,10 @@ class Batch:
                            "ms_block8": r[6]})
         return {"instances": int(v[0]), "dof": int(v[1]), "run_s": v[2],
                 "dof_steps": int(v[3]), "groups": groups}
+
+    def inject_wait_timeout(self, tile, spins=0):
+        """Test hook: tile `tile` of every group is skipped (see Handle)."""
+        _check(lib().sdg_batch_debug_inject_wait_timeout(self._b, tile, spins))
 
     def close(self):
         if self._b:

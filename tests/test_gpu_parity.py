@@ -109,7 +109,8 @@ def run_both(p, dims, nstep, flags, ev=orc.OPT1, vel_kind=1):
 
 
 @pytest.mark.parametrize("p,dims,nstep", [(1, (4, 3, 2), 40), (3, (4, 4, 3), 30),
-                                          (7, (3, 2, 4), 20), (10, (2, 2, 2), 8)])
+                                          (7, (3, 2, 4), 20), (10, (2, 2, 2), 8),
+                                          (12, (2, 2, 2), 4), (14, (2, 2, 2), 4)])
 def test_trajectory_fast(p, dims, nstep):
     got, ref = run_both(p, dims, nstep, 0)
     assert rel_maxnorm(got, ref) <= TOL
@@ -241,3 +242,25 @@ def test_partial_last_tile_and_uneven_sizes():
         ref = orc.cal_tend(orc.OPT1, q, u, v, w, ops, omesh)[:, : mesh.Ne]
         assert np.array_equal(got, ref), (p, dims)
         h.close()
+
+
+@pytest.mark.parametrize("p", [11, 12, 13, 14, 15])
+def test_fast_high_order_variants_agree(p):
+    """Fast FP64 at p = 11-15: the pipelined kernel at one block per SM (up
+    to the 227 KB plan of p = 14) and the one-tile-per-block kernel give the
+    same bits over RK steps, and both stay within 1e-12 of the oracle."""
+    dims, nstep = (2, 3, 2), 3
+    ops, mesh, omesh, (q, u, v, w) = case(p, dims)
+    dt = 0.1 / 3 / (p + 1) ** 2
+    res = []
+    for var in (sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE):
+        h = sdg.Handle(ops, mesh, 0)
+        h.set_kernel_variant(var)
+        h.set_state(q, u, v, w)
+        h.rk3_steps(dt, nstep)
+        res.append(h.get_field())
+        h.close()
+    assert np.array_equal(res[0], res[1])
+    qo = q.copy(order="F")
+    orc.run_rk3(orc.OPT1, qo, u, v, w, ops, omesh, dt, nstep)
+    assert rel_maxnorm(res[1], qo[:, : mesh.Ne]) <= TOL

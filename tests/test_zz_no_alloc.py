@@ -69,3 +69,28 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     assert rc == sdg.SDG_OK
     torch.cuda.synchronize()
     assert out.cpu().numpy().tolist() == [0.0, 0.0]
+
+
+@pytest.mark.parametrize("n", [1, 8193, 33554432])
+def test_noalloc_sizes_against_torch(n):
+    """Edge sizes: one value, a partial second block, and the capacity limit
+    (all 4,096 partial slots and the last-block fold), with planted extremes
+    in the first and the last block."""
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(n)
+    x = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    if n > 1:
+        x[n - 1] = 1e6        # maximum in the last (partial) block
+        x[3 % n] = -1e6       # minimum in the first block
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    for _ in range(2):        # the second call reuses the shared scratch
+        rc = sdg.lib().sdg_minmax_dev_noalloc(ctypes.c_void_p(x.data_ptr()), n,
+                                               ctypes.c_void_p(out.data_ptr()), None)
+        assert rc == sdg.SDG_OK
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        assert got[0] == float(x.min()) and got[1] == float(x.max()), (n, got)
+        x.neg_()              # new extremes for the second call
+    del x
+    torch.cuda.empty_cache()
