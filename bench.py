@@ -28,13 +28,16 @@ roofline, clocks and, for the mixed form, its accuracy):
   batch_fp64, batch_mixed  the 96-instance batched ensemble (Ne per axis
          U{6..24}, p in {3,5,7,9}), CUDA-graph RK steps, autotuned tiles;
   served  a short Poisson request stream at ~80 % load (--form-requests
-         requests; the served workload runs the long stream).
+         requests; the served workload runs the long stream), against the
+         same requests solved one at a time in plain FP64.
 --forms none skips them.
 
 Other workloads (--workload): fp64_8c_p3, mixed_32c_p7, mixed_16c_p15,
 batch_fp64, batch_mixed, served, divlike_var5_32c_p7 (the five-field
-derivative operator) and pscan (one instance of ~16.8 M DOF per order
-p = 1..15, FP64 and mixed, through the autotuned batch path).
+derivative operator), pscan (one instance of ~16.8 M DOF per order
+p = 1..15, FP64 and mixed, through the autotuned batch path) and
+zslab_fp64_32c_p7 (the 32^3 p = 7 mesh split into z-slabs over the N ranks,
+a halo exchange per stage; strong scaling).
 
 --impl reference runs the reference's CPU path (the oracle restatement; the
 Fortran reference cannot be compiled in this image) on all host threads, a
@@ -73,15 +76,17 @@ def parse(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="fp64_32c_p7",
                     choices=sorted(WORKLOADS) + ["batch_fp64", "batch_mixed", "served",
-                                                 "divlike_var5_32c_p7", "pscan"])
+                                                 "divlike_var5_32c_p7", "pscan",
+                                                 "zslab_fp64_32c_p7"])
     ap.add_argument("--forms", default="all", choices=["all", "none"],
                     help="headline run: also measure the mixed, batched and served forms")
     ap.add_argument("--requests", type=int, default=2000,
                     help="served workload: number of requests in the stream")
     ap.add_argument("--form-requests", type=int, default=40,
                     help="the served form of the default run: requests in its stream")
-    ap.add_argument("--seq-sample", type=int, default=12,
-                    help="served: requests solved one at a time for comparison")
+    ap.add_argument("--seq-sample", type=int, default=100,
+                    help="served workload: requests solved one at a time (plain FP64) "
+                         "for comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0,
                     help="budget of the CPU-baseline sample")
@@ -451,10 +456,11 @@ def time_batch(sdg, rep, mixed, steps, warmup, gidx, bf):
     gdof = {}
     for it in bf.comp:
         gdof[it["p"]] = gdof.get(it["p"], 0) + it["ne"] ** 3 * (it["p"] + 1) ** 3
-    names = {1: "block", 2: "pipe", 3: "block8"}
+    names = {1: "block", 2: "pipe", 3: "block8", 4: "split"}
     groups = []
     for g in info["groups"]:
-        ms = {"pipe": g["ms_pipe"], "block": g["ms_block"], "block8": g["ms_block8"]}
+        ms = {"pipe": g["ms_pipe"], "block": g["ms_block"], "block8": g["ms_block8"],
+              "split": g["ms_split"]}
         chosen = ms[names.get(g["variant"], "pipe")]
         gb = gdof[g["p"]] * bpd[1] / (chosen * 1e-3) / 1e9 if chosen > 0 else None
         groups.append({"p": g["p"], "dof": gdof[g["p"]], "tiles": g["tiles"],
@@ -641,8 +647,8 @@ def run_ours(args):
         forms["batch_fp64"]["vs_fp64_32c_p7"] = forms["batch_fp64"]["value"] / head["value"]
         forms["batch_mixed"]["vs_fp64_32c_p7"] = forms["batch_mixed"]["value"] / head["value"]
         del bf
-        forms["served"] = time_served(sdg, rep, args.form_requests,
-                                      min(args.seq_sample, 6), gidx)
+        forms["served"] = time_served(sdg, rep, args.form_requests, args.form_requests,
+                                      gidx)
 
     if rank == 0:
         line = {
@@ -718,6 +724,79 @@ def run_served(args):
     print(json.dumps(line), flush=True)
 
 
+def run_zslab(args):
+    """zslab_fp64_32c_p7: the 32^3 p = 7 FP64 mesh split into z-slabs over
+    the N ranks (strong scaling).  Each RK stage: the local update_halo of
+    the stage input, the exchange of the boundary layers with the two
+    neighbouring ranks (torch.distributed point-to-point; NCCL on GPUs) into
+    the z halo slots, then the stage kernel, which reads every boundary face
+    from the halo.  N = 1 runs the same path with the local periodic halo."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl", "cuda")
+    import sdg_b200 as sdg
+    from sdg_b200.zslab import ZSlab
+    NeX, NeY, NeZ, p = 32, 32, 32, 7
+    ops = sdg.read_operators(p)
+    sl = ZSlab(NeX, NeY, NeZ, p, ops.x1D, rank, world, sdg.mesh_setup)
+    gpos = sdg.mesh_setup(NeX, NeY, NeZ, p, ops.x1D)
+    fields = sdg.init_fields(gpos, **fields_kwargs((1.0, 0.5, 0.25)))
+    del gpos
+    H = sdg.Handle(ops, sl.mesh, sdg.FLAG_EXTERNAL_HALO)
+    H.set_state(*(sl.local(f) for f in fields))
+    del fields
+    dt = dt_for(NeZ, p)
+    hs = torch.cuda.ExternalStream(H.stream())
+    dist = rep.pg
+
+    def exchange(t):
+        if dist is not None:
+            sl.exchange(t, dist, lambda n: torch.empty(n, dtype=t.dtype, device=t.device))
+
+    with torch.cuda.stream(hs):
+        for which in (sdg.FIELD_U, sdg.FIELD_V, sdg.FIELD_W):
+            exchange(H.resident_array(which))
+    stage_in = [H.stage_input(s) for s in (1, 2, 3)]
+
+    def step():
+        with torch.cuda.stream(hs):
+            for s in (1, 2, 3):
+                H.update_halo_stage(s)
+                exchange(stage_in[s - 1])
+                H.rk3_stage(s, dt)
+
+    for _ in range(args.warmup):
+        step()
+    H.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_index(local)) as clk:
+        rep.barrier()
+        ev0.record(hs)
+        for _ in range(args.steps):
+            step()
+        ev1.record(hs)
+        H.synchronize()
+        rep.barrier()
+    t = rep.max(ev0.elapsed_time(ev1) * 1e-3)
+    dof = NeX * NeY * NeZ * (p + 1) ** 3
+    H.close()
+    rep.close()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": METRIC, "value": dof * 3 * args.steps / t, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "zslab_fp64_32c_p7", "mesh": [NeX, NeY, NeZ], "p": p,
+                   "dof_total": dof, "slabs": world,
+                   "exchange_bytes_per_stage_per_rank": 2 * NeX * NeY * (p + 1) ** 2 * 8,
+                   "parallelism": f"zslab{world}"},
+        "clocks": clk.summary(), "gpu_launches": 6 * args.steps}), flush=True)
+
+
 def run_pscan(args):
     """Per-order map: for p = 1..15, one periodic box of ~16.8 M DOF, FP64 and
     mixed, autotuned through the batch path; K RK3 steps each.  frac uses the
@@ -728,7 +807,7 @@ def run_pscan(args):
     rep = Replicas("nccl", "cuda")
     import sdg_b200 as sdg
     peak, peak_kind = measured_peaks()
-    names = {1: "Block", 2: "Pipe", 3: "BlockOcc"}
+    names = {1: "Block", 2: "Pipe", 3: "BlockOcc", 4: "Split"}
     rows = []
     for mixed in (False, True):
         for p in range(1, 16):
@@ -755,7 +834,7 @@ def run_pscan(args):
                          "G_dof_updates_per_s": G / 1e9, "frac": G * bpd / 1e9 / peak,
                          "variant": names.get(g["variant"], g["variant"]),
                          "stage2_ms": {"pipe": g["ms_pipe"], "block": g["ms_block"],
-                                       "block8": g["ms_block8"]}})
+                                       "block8": g["ms_block8"], "split": g["ms_split"]}})
     rep.close()
     if rank != 0:
         return
@@ -890,6 +969,8 @@ def main():
         run_derivative(args)
     elif args.workload == "pscan":
         run_pscan(args)
+    elif args.workload == "zslab_fp64_32c_p7":
+        run_zslab(args)
     elif args.workload != "fp64_32c_p7":
         run_mesh_only(args)
     else:

@@ -50,12 +50,23 @@ extern "C" {
 #define SDG_FLAG_MIXED 4          /* resident RK path in mixed precision:
                                      FP32 velocity, tendency and stage
                                      intermediates, FP64 RK accumulation   */
+#define SDG_FLAG_EXTERNAL_HALO 8  /* resident path for a subdomain: every
+                                     boundary face reads its plus side from
+                                     the halo region of the stage input, and
+                                     the caller fills that halo before each
+                                     sdg_rk3_stage (sdg_update_halo_stage plus
+                                     its own exchange, e.g. of z-slabs);
+                                     sdg_rk3_steps is then unavailable       */
 
 /* Fields for sdg_set_field / sdg_get_field. */
 #define SDG_FIELD_Q 0
 #define SDG_FIELD_U 1
 #define SDG_FIELD_V 2
 #define SDG_FIELD_W 3
+/* Further resident arrays for sdg_resident_array: the inputs of RK stages 2
+ * and 3 (stage 1 reads SDG_FIELD_Q). */
+#define SDG_ARRAY_STAGE2 4
+#define SDG_ARRAY_STAGE3 5
 
 typedef struct sdg_handle sdg_handle;
 
@@ -190,6 +201,21 @@ int sdg_synchronize(sdg_handle* h);
 /* Device pointer of a resident field (SDG_FIELD_Q gives the FP64 state). */
 int sdg_field_dev_ptr(sdg_handle* h, int which, void** ptr);
 
+/* A resident (Np, NeA) device array as the kernels read it: SDG_FIELD_Q
+ * (FP64 state, the input of RK stage 1), SDG_FIELD_U/V/W (velocity at the
+ * compute precision) or SDG_ARRAY_STAGE2/3 (inputs of stages 2 and 3);
+ * *elem_bytes receives 8 (FP64) or 4 (FP32).  For callers that fill halos
+ * themselves (SDG_FLAG_EXTERNAL_HALO): the halo region of each array starts
+ * at element Np*Ne.  Replaces the halo buffer of mod_mesh.f90:119-130 as the
+ * landing zone of a domain-decomposition exchange. */
+int sdg_resident_array(sdg_handle* h, int which, void** ptr, int* elem_bytes);
+
+/* update_halo (mod_mesh.f90:209-221) of the input array of RK stage
+ * `stage` (1..3) from this subdomain's own halo_src_map, on the handle's
+ * stream.  With SDG_FLAG_EXTERNAL_HALO the caller then overwrites the slots
+ * that belong to other subdomains and calls sdg_rk3_stage. */
+int sdg_update_halo_stage(sdg_handle* h, int stage);
+
 /* Accumulated device time in seconds: t[0] = tendency/stage kernels of
  * sdg_cal_tend*, t[1] = sdg_rk3_steps, t[2] = halo updates, t[3] = copies
  * of sdg_cal_tend (host<->device). */
@@ -199,9 +225,12 @@ int sdg_timers(sdg_handle* h, double* t4);
 long long sdg_launch_count(sdg_handle* h);
 
 /* Selects the fused-kernel variant: 0 = automatic (default; also set by the
- * environment variable SDG_KERNEL=block|pipe at sdg_init), 1 = one element
- * tile per block, 2 = persistent blocks with a bulk-copy (TMA) ring.  Both
- * compute identical results; the choice only affects speed. */
+ * environment variable SDG_KERNEL=block|pipe|blockocc|split at sdg_init),
+ * 1 = one element tile per block, 2 = persistent blocks with a bulk-copy
+ * (TMA) ring, 3 = one tile per block built for 8 resident blocks (p = 3..7),
+ * 4 = the bulk-copy ring with each z-column split over two threads (p >= 8;
+ * other orders run variant 2).  All compute identical results; the choice
+ * only affects speed. */
 int sdg_set_kernel_variant(sdg_handle* h, int variant);
 
 /* Test hook for the failure path of the bounded waits (no reference
@@ -254,7 +283,8 @@ int sdg_batch_get(sdg_batch* b, int id, double* q);
 
 /* Up to n values: instances, total DOF, run seconds, DOF x steps run,
  * groups, then per group p, mixed, tiles, chosen variant and the tuned
- * stage times (ms) of the pipelined, block and 8-blocks-per-SM variants.
+ * stage times (ms) of the pipelined, block, 8-blocks-per-SM and
+ * split-column variants (0 where not a candidate).
  * Returns the number of values available. */
 int sdg_batch_info(sdg_batch* b, double* out, int n);
 

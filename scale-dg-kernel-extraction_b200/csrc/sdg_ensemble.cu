@@ -158,7 +158,7 @@ struct Group {
   std::vector<BatchTile> h_tiles;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
-  double tuned_ms[4] = {0, 0, 0, 0};
+  double tuned_ms[5] = {0, 0, 0, 0, 0};  // by KernelVariant
 };
 
 struct Ensemble {
@@ -440,7 +440,7 @@ struct Ensemble {
     if (g->members.empty()) return SDG_OK;
     LaunchSpec l = spec(g, st, s);
     l.variant = variant;
-    if (variant == kVariantPipe) {
+    if (variant == kVariantPipe || variant == kVariantSplit) {
       l.batch_insts = g->d_insts + st * g->inst_cap;
       l.batch_tiles = g->d_tiles;
       l.batch_ntiles = g->ntiles;
@@ -504,6 +504,11 @@ struct Ensemble {
                             pipe_supported(g->nq, g->mixed ? kStageMixed1 : kStageF64) &&
                             pipe_supported(g->nq, g->mixed ? kStageMixed3 : kStageF64);
       if (can_pipe) cands.push_back(kVariantPipe);
+      const bool can_split = split_supported(g->nq, g->mixed ? kStageMixed2 : kStageF64) &&
+                             split_supported(g->nq, g->mixed ? kStageMixed1 : kStageF64) &&
+                             split_supported(g->nq, g->mixed ? kStageMixed3 : kStageF64) &&
+                             ((g->flags & SDG_FLAG_EXACT) || !g->ops->lift_z.empty());
+      if (can_split) cands.push_back(kVariantSplit);
       cands.push_back(kVariantBlock);
       if (g->nq >= 4 && g->nq <= 8) cands.push_back(kVariantBlockOcc);
       cudaEvent_t e0, e1;
@@ -522,7 +527,7 @@ struct Ensemble {
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
         const double t = ms / reps;
-        if (v >= 0 && v < 4) g->tuned_ms[v] = t;
+        if (v >= 0 && v < 5) g->tuned_ms[v] = t;
         if (t < best) {
           best = t;
           best_v = v;
@@ -546,7 +551,7 @@ struct Ensemble {
       for (int st = 0; st < 3; ++st) {
         LaunchSpec l = spec(g, st, g->stream);
         l.variant = g->variant;
-        if (g->variant == kVariantPipe) {
+        if (g->variant == kVariantPipe || g->variant == kVariantSplit) {
           l.batch_insts = g->d_insts;
           l.batch_tiles = g->d_tiles;
           l.batch_ntiles = 0;
@@ -721,7 +726,8 @@ int sdg_batch_get(sdg_batch* b, int id, double* q) {
 
 int sdg_batch_info(sdg_batch* b, double* out, int n) {
   // out: [instances, total DOF, run seconds, DOF-steps run, groups,
-  //       then per group (p, mixed, tiles, variant, t_pipe, t_block, t_block8)]
+  //       then per group (p, mixed, tiles, variant, t_pipe, t_block, t_block8,
+  //       t_split)]
   if (!b || !out) return fail(SDG_ERR_ARG, "null argument");
   std::vector<double> v;
   long long dof = 0;
@@ -740,6 +746,7 @@ int sdg_batch_info(sdg_batch* b, double* out, int n) {
     v.push_back(g->tuned_ms[kVariantPipe]);
     v.push_back(g->tuned_ms[kVariantBlock]);
     v.push_back(g->tuned_ms[kVariantBlockOcc]);
+    v.push_back(g->tuned_ms[kVariantSplit]);
   }
   for (int i = 0; i < n && i < static_cast<int>(v.size()); ++i) out[i] = v[i];
   return static_cast<int>(v.size());
@@ -773,13 +780,25 @@ int sdg_batch_destroy(sdg_batch* b) {
 // ===========================================================================
 // Serving loop
 // ===========================================================================
-// A worker thread owns the GPU side.  Each iteration it (1) admits queued
-// requests while their device memory fits under the byte cap, (2) advances
-// every admitted request by one SSP-RK3 step - all orders and sizes in one
-// fork/join of batched launches - and (3) retires requests whose steps are
-// done (result copied to the host, memory returned to the pool).  Requests
-// that arrive while others run join at the next step boundary, so their
-// work overlaps the others' on the device.
+// A worker thread owns the GPU side and advances the admitted requests in
+// chunks of RK steps.  Each chunk replays the CUDA graph of one RK step of
+// the current membership (all orders and sizes in one fork/join of batched
+// launches) n times, n = min(kChunkSteps, the fewest steps any member has
+// left), so no member overruns and the host meets the GPU once per chunk,
+// not once per step.  While a chunk runs, the worker
+//   * admits queued requests in arrival order while their device memory
+//     fits under the byte cap, uploading them on a copy stream of their own
+//     (the running chunk is not stalled by the uploads), and
+//   * copies out the results of the requests that the previous chunk
+//     finished, again on the copy stream, and returns their memory.
+// At the chunk boundary it reads the status word of the bounded waits once,
+// updates the membership (finished requests leave, admitted ones join),
+// re-captures the step graph if the membership changed, and launches the
+// next chunk.  Requests that arrive while others run join at the next chunk
+// boundary, so their work overlaps the others' on the device.
+constexpr int kChunkSteps = 16;
+constexpr double kChunkMs = 8.0;
+
 // Operators submitted with a request, kept until its admission (ops_for
 // needs the arrays).
 struct PendingOps {
@@ -794,7 +813,7 @@ struct sdg_server {
   std::condition_variable cv;      // work arrived / stop
   std::condition_variable done_cv; // a request finished
   std::deque<Inst*> queue;
-  std::vector<Inst*> active;
+  std::vector<Inst*> active;       // members of the running chunk's graph
   std::map<int, std::unique_ptr<Inst>> all;
   // Operators of queued requests, by request (guarded by mu, like queue).
   std::map<const Inst*, PendingOps> pending_ops;
@@ -803,9 +822,34 @@ struct sdg_server {
   int error = SDG_OK;
   std::string error_msg;
   std::thread worker;
-  double busy = 0;            // seconds of device steps
+  double busy = 0;            // seconds of device time of the chunks
   long long dof_steps = 0;    // DOF x RK steps completed
-  long long steps_run = 0;
+  long long steps_run = 0;    // RK steps run (over all chunks)
+  long long chunks = 0;
+
+  // Worker-only state (no lock needed).
+  cudaStream_t copy = nullptr;       // uploads and result downloads
+  cudaGraphExec_t graph = nullptr;   // one RK step of `active`
+  bool graph_stale = true;
+  cudaEvent_t c0 = nullptr, c1 = nullptr;  // brackets of the running chunk
+  bool chunk_running = false;
+  int chunk_steps = 0;
+  double step_ms = 0;                // device time per step of the last chunk
+  std::vector<Inst*> joining;        // admitted, uploaded, not yet members
+
+  ~sdg_server() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (c0) cudaEventDestroy(c0);
+    if (c1) cudaEventDestroy(c1);
+    if (copy) cudaStreamDestroy(copy);
+  }
+
+  int init_worker_state() {
+    ENS_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+    ENS_CUDA(cudaEventCreate(&c0));
+    ENS_CUDA(cudaEventCreate(&c1));
+    return SDG_OK;
+  }
 
   void loop() {
     cudaSetDevice(ens.dev);
@@ -813,7 +857,10 @@ struct sdg_server {
       std::vector<Inst*> admit;
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv.wait(lk, [&] { return stop || !queue.empty() || !active.empty(); });
+        cv.wait(lk, [&] {
+          return stop || !queue.empty() || !active.empty() || !joining.empty() ||
+                 chunk_running;
+        });
         if (stop) return;
         while (!queue.empty() && used + queue.front()->bytes <= cap) {
           Inst* I = queue.front();
@@ -824,15 +871,40 @@ struct sdg_server {
       }
       // Only this thread touches the ensemble (operators, groups, device
       // memory); submitters only touch the queue under the lock.
-      if (!step_once(admit)) return;
+      admit_requests(admit);
+      finish_chunk();
+      launch_chunk();
     }
   }
 
-  bool step_once(std::vector<Inst*>& admit);
+  void fail_all(int rc);
+  void admit_requests(std::vector<Inst*>& admit);
+  void finish_chunk();
+  void launch_chunk();
 };
 
-bool sdg_server::step_once(std::vector<Inst*>& admit) {
-  // Admission: allocate, upload, join the order's group.
+// Fails every request on the device after an error (the worker keeps
+// serving later submissions).
+void sdg_server::fail_all(int rc) {
+  std::lock_guard<std::mutex> lk(mu);
+  error = rc;
+  error_msg = last_error();
+  for (auto* list : {&active, &joining})
+    for (Inst* I : *list) {
+      ens.leave(I);
+      ens.release(I, ens.stream);
+      used -= I->bytes;
+      I->state = kFailed;
+    }
+  active.clear();
+  joining.clear();
+  graph_stale = true;
+  done_cv.notify_all();
+}
+
+// Uploads the admitted requests on the copy stream (the running chunk goes
+// on) and queues them to join at the next chunk boundary.
+void sdg_server::admit_requests(std::vector<Inst*>& admit) {
   for (Inst* I : admit) {
     int rc;
     Ops* o = nullptr;
@@ -846,7 +918,7 @@ bool sdg_server::step_once(std::vector<Inst*>& admit) {
     rc = ens.ops_for(I->p, po.D.data(), po.L.data(), &o);
     if (!rc) rc = ens.group_for(I->nq, I->mixed, o, &g);
     if (!rc) rc = ens.upload(I, I->host[0].data(), I->host[1].data(), I->host[2].data(),
-                             I->host[3].data(), ens.stream);
+                             I->host[3].data(), copy);
     std::lock_guard<std::mutex> lk(mu);
     if (rc) {
       I->state = kFailed;
@@ -859,56 +931,142 @@ bool sdg_server::step_once(std::vector<Inst*>& admit) {
     for (auto& h : I->host) std::vector<double>().swap(h);
     I->state = kRunning;
     I->t_admit = now_s();
-    ens.join(I, g);
-    active.push_back(I);
+    joining.push_back(I);
   }
-  if (active.empty()) return true;
-  // One RK step of everything admitted.
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventRecord(e0, ens.stream);
-  int rc = ens.step(ens.stream);
-  cudaEventRecord(e1, ens.stream);
-  cudaError_t ce = cudaEventSynchronize(e1);
-  float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (!rc && ce != cudaSuccess) rc = fail(SDG_ERR_CUDA, "serving step failed: %s",
-                                          cudaGetErrorString(ce));
-  if (!rc) rc = ens.check_status();
-  std::lock_guard<std::mutex> lk(mu);
-  busy += 1e-3 * ms;
-  ++steps_run;
-  if (rc) {
-    error = rc;
-    error_msg = last_error();
-    for (Inst* I : active) I->state = kFailed;
-    active.clear();
-    done_cv.notify_all();
-    return true;
-  }
-  // Retire finished requests.
-  std::vector<Inst*> keep;
-  for (Inst* I : active) {
-    dof_steps += static_cast<long long>(I->np) * I->ne;
-    if (--I->steps_left > 0) {
-      keep.push_back(I);
-      continue;
+}
+
+// Waits for the running chunk, accounts it, retires the members it
+// finished (results copied out on the copy stream, memory returned) and
+// lets the admitted requests join.
+void sdg_server::finish_chunk() {
+  if (chunk_running) {
+    cudaError_t ce = cudaEventSynchronize(c1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c0, c1);
+    int rc = ce == cudaSuccess ? SDG_OK
+                               : fail(SDG_ERR_CUDA, "serving chunk failed: %s",
+                                      cudaGetErrorString(ce));
+    if (!rc) rc = ens.check_status();
+    if (chunk_steps > 0) step_ms = ms / chunk_steps;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      busy += 1e-3 * ms;
+      steps_run += chunk_steps;
+      ++chunks;
+      if (rc) chunk_running = false;
     }
-    I->result.resize(static_cast<size_t>(I->np) * I->ne);
-    cudaMemcpy(I->result.data(), I->q0, I->result.size() * sizeof(double),
-               cudaMemcpyDeviceToHost);
-    ens.leave(I);
-    ens.release(I, ens.stream);
-    used -= I->bytes;
-    I->t_done = now_s();
-    I->state = kDone;
+    if (rc) {
+      fail_all(rc);
+      return;
+    }
+    std::vector<Inst*> keep, done;
+    long long dof = 0;
+    for (Inst* I : active) {
+      dof += static_cast<long long>(I->np) * I->ne;
+      I->steps_left -= chunk_steps;
+      (I->steps_left > 0 ? keep : done).push_back(I);
+    }
+    for (Inst* I : done) {
+      ens.leave(I);
+      graph_stale = true;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu);  // `active` is read by sdg_serve_wait
+      active.swap(keep);
+    }
+    // Results of the finished members, then their memory, on the copy
+    // stream; the next chunk (compute stream) no longer touches them.
+    for (Inst* I : done) {
+      I->result.resize(static_cast<size_t>(I->np) * I->ne);
+      cudaMemcpyAsync(I->result.data(), I->q0, I->result.size() * sizeof(double),
+                      cudaMemcpyDeviceToHost, copy);
+      ens.release(I, copy);
+    }
+    if (!done.empty()) cudaStreamSynchronize(copy);
+    std::lock_guard<std::mutex> lk(mu);
+    dof_steps += dof * chunk_steps;
+    for (Inst* I : done) {
+      used -= I->bytes;
+      I->t_done = now_s();
+      I->state = kDone;
+    }
+    chunk_running = false;
+    done_cv.notify_all();
   }
-  active.swap(keep);
-  done_cv.notify_all();
-  return true;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!joining.empty()) {
+    for (Inst* I : joining) {
+      Group* g = ens.groups.at(std::make_pair(I->nq, I->mixed)).get();
+      ens.join(I, g);
+      active.push_back(I);
+    }
+    joining.clear();
+    graph_stale = true;
+  }
+}
+
+// Re-captures the step graph if the membership changed and launches the
+// next chunk: as many steps as fit in about kChunkMs of device time at the
+// last measured step time (at most kChunkSteps, at least one), so that a
+// request that arrives meanwhile waits at most about that long to join.
+void sdg_server::launch_chunk() {
+  if (active.empty()) {
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    return;
+  }
+  int rc = SDG_OK;
+  if (graph_stale) {
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    // Tables and the kernels' one-time set-up outside the capture.
+    rc = ens.prime();
+    cudaGraph_t gr = nullptr;
+    if (!rc) {
+      cudaError_t e = cudaStreamBeginCapture(ens.stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        rc = fail(SDG_ERR_CUDA, "serving graph capture: %s", cudaGetErrorString(e));
+      } else {
+        rc = ens.step(ens.stream);
+        e = cudaStreamEndCapture(ens.stream, &gr);
+        if (!rc && e != cudaSuccess)
+          rc = fail(SDG_ERR_CUDA, "serving graph capture: %s", cudaGetErrorString(e));
+      }
+    }
+    if (!rc) {
+      cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
+      if (e != cudaSuccess)
+        rc = fail(SDG_ERR_CUDA, "serving graph instantiate: %s", cudaGetErrorString(e));
+    }
+    if (gr) cudaGraphDestroy(gr);
+    if (rc) {
+      fail_all(rc);
+      return;
+    }
+    graph_stale = false;
+  }
+  long long n = kChunkSteps;
+  if (step_ms > 0) n = std::max(1LL, std::min(n, static_cast<long long>(kChunkMs / step_ms)));
+  for (Inst* I : active) n = std::min(n, I->steps_left);
+  chunk_steps = static_cast<int>(n);
+  cudaEventRecord(c0, ens.stream);
+  for (int k = 0; k < chunk_steps && !rc; ++k) {
+    cudaError_t e = cudaGraphLaunch(graph, ens.stream);
+    if (e != cudaSuccess)
+      rc = fail(SDG_ERR_CUDA, "serving graph launch: %s", cudaGetErrorString(e));
+  }
+  cudaEventRecord(c1, ens.stream);
+  if (rc) {
+    cudaStreamSynchronize(ens.stream);
+    fail_all(rc);
+    return;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  chunk_running = true;
 }
 
 extern "C" {
@@ -924,6 +1082,7 @@ int sdg_serve_create(sdg_server** out, double max_bytes) {
   // Default cap: 85% of the device memory free now.
   s->cap = max_bytes > 0 ? static_cast<size_t>(max_bytes)
                          : static_cast<size_t>(0.85 * static_cast<double>(free_b));
+  if ((rc = s->init_worker_state())) return rc;
   sdg_server* raw = s.release();
   raw->worker = std::thread([raw] { raw->loop(); });
   *out = raw;
@@ -1000,7 +1159,9 @@ int sdg_serve_wait(sdg_server* s, double timeout_s) {
   std::unique_lock<std::mutex> lk(s->mu);
   const auto deadline = std::chrono::steady_clock::now() +
                         std::chrono::duration<double>(timeout_s > 0 ? timeout_s : 1e9);
-  auto idle = [&] { return s->queue.empty() && s->active.empty(); };
+  auto idle = [&] {
+    return s->queue.empty() && s->active.empty() && s->joining.empty() && !s->chunk_running;
+  };
   if (!s->done_cv.wait_until(lk, deadline, idle))
     return fail(SDG_ERR_STATE, "requests still pending after %.1f s", timeout_s);
   if (s->error) return fail(s->error, "%s", s->error_msg.c_str());
@@ -1027,7 +1188,9 @@ int sdg_serve_destroy(sdg_server* s) {
   }
   if (s->worker.joinable()) s->worker.join();
   cudaSetDevice(s->ens.dev);
+  cudaStreamSynchronize(s->ens.stream);
   for (Inst* I : s->active) s->ens.release(I, s->ens.stream);
+  for (Inst* I : s->joining) s->ens.release(I, s->ens.stream);
   cudaStreamSynchronize(s->ens.stream);
   delete s;
   return SDG_OK;

@@ -39,7 +39,12 @@ int pipe_elems_per_tile(int nq) {
 
 bool pipe_supported(int nq, int kind) {
   int epb = 1;
-  return pipe_info(nq, kind, &epb) != 0;
+  return (pipe_info(nq, kind, &epb) & 1) != 0;
+}
+
+bool split_supported(int nq, int kind) {
+  int epb = 1;
+  return (pipe_info(nq, kind, &epb) & 2) != 0;
 }
 
 int launch_tend(const LaunchSpec& s) {
@@ -394,7 +399,9 @@ int compress_tables(sdg_handle* h, const int* VMapM, const int* VMapP,
       }
     }
   }
-  h->direct_ok = direct;
+  // A subdomain whose halo the caller fills reads every boundary face
+  // through the halo.
+  h->direct_ok = direct && !(h->flags & SDG_FLAG_EXTERNAL_HALO);
   return SDG_OK;
 }
 
@@ -436,7 +443,7 @@ int enqueue_stage(sdg_handle* h, int st, double dt) {
   const double rb[3] = {1.0, 0.25, 2.0 / 3.0};
   const void* in[3] = {h->q0, h->qa, h->qb};
   void* out[3] = {h->qa, h->qb, h->q0};
-  if (!h->direct_ok) {
+  if (!h->direct_ok && !(h->flags & SDG_FLAG_EXTERNAL_HALO)) {
     const bool in32 = f32 && st > 0;
     int rc = launch_halo(h, const_cast<void*>(in[st]), in32, h->stream);
     if (rc) return rc;
@@ -528,7 +535,8 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
   if (!D1D || !Lift_mat || !VMapM || !VMapP || !normal_fn || !Escale || !Fscale ||
       (NhaloNode > 0 && !halo_src_map))
     return fail(SDG_ERR_ARG, "sdg_init: null array argument");
-  if (flags & ~(SDG_FLAG_EXACT | SDG_FLAG_ORDER_GENERAL | SDG_FLAG_MIXED))
+  if (flags & ~(SDG_FLAG_EXACT | SDG_FLAG_ORDER_GENERAL | SDG_FLAG_MIXED |
+                SDG_FLAG_EXTERNAL_HALO))
     return fail(SDG_ERR_ARG, "sdg_init: unknown flag bits 0x%x", flags);
   if ((flags & SDG_FLAG_MIXED) && (flags & SDG_FLAG_EXACT))
     return fail(SDG_ERR_ARG, "SDG_FLAG_EXACT applies to the FP64 form only");
@@ -572,6 +580,7 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
     if (kv && std::strcmp(kv, "block") == 0) h->variant = kVariantBlock;
     else if (kv && std::strcmp(kv, "pipe") == 0) h->variant = kVariantPipe;
     else if (kv && std::strcmp(kv, "blockocc") == 0) h->variant = kVariantBlockOcc;
+    else if (kv && std::strcmp(kv, "split") == 0) h->variant = kVariantSplit;
   }
 
   auto bail = [&](int code) { free_handle(h); return code; };
@@ -743,6 +752,9 @@ int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps) {
   if (nsteps < 0) return fail(SDG_ERR_ARG, "nsteps must be >= 0");
   if (!h->have_q || !h->have_vel[0] || !h->have_vel[1] || !h->have_vel[2])
     return fail(SDG_ERR_STATE, "upload q, u, v and w with sdg_set_field first");
+  if (h->flags & SDG_FLAG_EXTERNAL_HALO)
+    return fail(SDG_ERR_STATE, "SDG_FLAG_EXTERNAL_HALO: the caller fills the halo between "
+                "stages; run sdg_update_halo_stage, the exchange and sdg_rk3_stage");
   if (nsteps == 0) return SDG_OK;
   if ((rc = prime_stages(h))) return rc;
   if (!h->graph || h->graph_dt != dt) {
@@ -849,6 +861,28 @@ int sdg_field_dev_ptr(sdg_handle* h, int which, void** ptr) {
   return SDG_OK;
 }
 
+int sdg_resident_array(sdg_handle* h, int which, void** ptr, int* elem_bytes) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (!ptr || which < SDG_FIELD_Q || which > SDG_ARRAY_STAGE3)
+    return fail(SDG_ERR_ARG, "sdg_resident_array: bad argument");
+  if ((rc = ensure_state(h))) return rc;
+  const int es = mixed(h) ? 4 : 8;
+  void* arrays[6] = {h->q0, h->vel[0], h->vel[1], h->vel[2], h->qa, h->qb};
+  *ptr = arrays[which];
+  if (elem_bytes) *elem_bytes = which == SDG_FIELD_Q ? 8 : es;
+  return SDG_OK;
+}
+
+int sdg_update_halo_stage(sdg_handle* h, int stage) {
+  int rc = check_handle(h);
+  if (rc) return rc;
+  if (stage < 1 || stage > 3) return fail(SDG_ERR_ARG, "stage must be 1..3");
+  if ((rc = ensure_state(h))) return rc;
+  void* in[3] = {h->q0, h->qa, h->qb};
+  return launch_halo(h, in[stage - 1], mixed(h) && stage > 1, h->stream);
+}
+
 int sdg_timers(sdg_handle* h, double* t4) {
   if (!h || !t4) return fail(SDG_ERR_ARG, "null argument");
   account_rk(h);
@@ -863,9 +897,9 @@ long long sdg_launch_count(sdg_handle* h) { return h ? h->launches : -1; }
 
 int sdg_set_kernel_variant(sdg_handle* h, int variant) {
   if (!h) return fail(SDG_ERR_ARG, "null handle");
-  if (variant < kVariantAuto || variant > kVariantBlockOcc)
-    return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block), 2 (pipelined) "
-                "or 3 (block, 8 blocks per SM)");
+  if (variant < kVariantAuto || variant > kVariantSplit)
+    return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block), 2 (pipelined), "
+                "3 (block, 8 blocks per SM) or 4 (pipelined, split columns)");
   if (variant != h->variant && h->graph) {
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;

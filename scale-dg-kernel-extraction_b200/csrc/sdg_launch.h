@@ -100,6 +100,9 @@ int pipe_elems_per_tile(int nq);
 // shared-memory plan fits).
 bool pipe_supported(int nq, int kind);
 
+// Whether the split-column kernel exists at this order and its plan fits.
+bool split_supported(int nq, int kind);
+
 // Launches the fused kernel described by `s`; returns SDG_OK or an SDG_ERR_*
 // status with the thread's last error set.
 int launch_tend(const LaunchSpec& s);
@@ -110,11 +113,15 @@ int launch_tend(const LaunchSpec& s);
 // one block (kPipeMaxSmem) and every array is 16-byte aligned.
 // kVariantBlockOcc is the one-tile-per-block kernel built for eight resident
 // blocks per SM (p = 3..7; other orders use kVariantBlock).
+// kVariantSplit is the persistent ring kernel with each z-column split over
+// two threads (tend_split_kernel), for the orders with one element per tile
+// (Nq >= 9).
 enum KernelVariant {
   kVariantAuto = 0,
   kVariantBlock = 1,
   kVariantPipe = 2,
-  kVariantBlockOcc = 3
+  kVariantBlockOcc = 3,
+  kVariantSplit = 4
 };
 
 // Returns 0 when launched, -1 when this unit does not hold spec.nq,
@@ -135,8 +142,9 @@ int launch_tend_nq14(const LaunchSpec&);
 int launch_tend_nq15(const LaunchSpec&);
 int launch_tend_nq16(const LaunchSpec&);
 
-// Per order: elements per tile of the pipelined kernel (*epb) and whether
-// its shared-memory plan fits for `kind` (return value).
+// Per order: elements per tile of the pipelined kernel (*epb) and which
+// persistent kernels' shared-memory plans fit for `kind` (return value: bit 0
+// the pipelined kernel, bit 1 the split-column kernel).
 int pipe_info_nq2(int kind, int* epb);
 int pipe_info_nq3(int kind, int* epb);
 int pipe_info_nq4(int kind, int* epb);

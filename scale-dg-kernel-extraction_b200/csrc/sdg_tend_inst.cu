@@ -8,6 +8,7 @@
 #include "sdg_launch.h"
 #include "sdg_tend.cuh"
 #include "sdg_tend_pipe.cuh"
+#include "sdg_tend_split.cuh"
 
 #ifndef SDG_NQ
 #error "SDG_NQ must be defined"
@@ -24,7 +25,7 @@ constexpr int NQ = SDG_NQ;
 // kernel is a template argument so that the set-up state belongs to that
 // kernel: kernels of one signature (tendency and stage forms) differ in
 // their shared-memory plans.
-template <auto KERN, typename Args, typename Dm>
+template <auto KERN, int THREADS = PipeGeo<NQ>::THREADS, typename Args, typename Dm>
 int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, const Dm& d) {
   constexpr auto kern = KERN;
   static DeviceSetup setup;  // blocks per SM, per kernel and device
@@ -37,14 +38,14 @@ int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, con
     if (e != cudaSuccess) return static_cast<int>(e);
     cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     int nb = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, PipeGeo<NQ>::THREADS, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, THREADS, smem);
     if (e != cudaSuccess) return static_cast<int>(e);
     blocks_per_sm = nb > 0 ? nb : 1;
     setup.slot[dev].store(blocks_per_sm, std::memory_order_relaxed);
   }
   if (ntiles <= 0) return 0;
   const int grid = std::min(ntiles, blocks_per_sm * (s.num_sms > 0 ? s.num_sms : 148));
-  kern<<<grid, PipeGeo<NQ>::THREADS, smem, s.stream>>>(a, d);
+  kern<<<grid, THREADS, smem, s.stream>>>(a, d);
   return static_cast<int>(cudaGetLastError());
 }
 
@@ -90,9 +91,33 @@ int run(const LaunchSpec& s) {
                         (EXACT || s.lift_z != nullptr) &&
                         (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
                                    aligned(s.w) && aligned(s.escale) && aligned(s.fscale)));
+  // The split-column kernel: orders with one element per tile.
+  if constexpr (NQ >= 9) {
+    constexpr int H = kSplitH<NQ>;
+    using SP = SplitPlan<NQ, H, TQ, TV, TC, STAGE>;
+    const bool can_split = SP::BYTES <= kPipeMaxSmem && SP::BYTES <= device_smem_optin() &&
+                           (EXACT || s.lift_z != nullptr) &&
+                           (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
+                                      aligned(s.w) && aligned(s.escale) &&
+                                      aligned(s.fscale)));
+    if (s.variant == kVariantSplit) {
+      if (!can_split) {
+        if (batch) return static_cast<int>(cudaErrorNotSupported);
+      } else {
+        constexpr int T = SplitGeo<NQ, H>::THREADS;
+        const int ntiles = batch ? s.batch_ntiles : s.nelem;
+        if (batch)
+          return launch_pipe<tend_split_kernel<NQ, H, TQ, TV, TO, TC, EXACT, ORDER, STAGE, true>,
+                             T>(SP::BYTES, ntiles, s, a, d);
+        return launch_pipe<tend_split_kernel<NQ, H, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false>,
+                           T>(SP::BYTES, ntiles, s, a, d);
+      }
+    }
+  }
   if (batch && !can_pipe) return static_cast<int>(cudaErrorNotSupported);
   const bool pipe =
-      batch || ((s.variant == kVariantPipe || s.variant == kVariantAuto) && can_pipe);
+      batch || ((s.variant == kVariantPipe || s.variant == kVariantAuto ||
+                 s.variant == kVariantSplit) && can_pipe);
   if (pipe) {
     const int ntiles =
         batch ? s.batch_ntiles : (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
@@ -158,12 +183,19 @@ int run(const LaunchSpec& s) {
 #define SDG_CAT2(a, b) a##b
 #define SDG_CAT(a, b) SDG_CAT2(a, b)
 
-// Whether the plan fits both the build's limit and the current device's
-// per-block opt-in.
+// Which persistent plans fit both the build's limit and the current
+// device's per-block opt-in: bit 0 the pipelined kernel, bit 1 the
+// split-column kernel (orders with one element per tile).
 template <typename TQ, typename TV, typename TC, bool STAGE>
-bool pipe_fits() {
+int pipe_fits() {
+  const size_t optin = device_smem_optin();
   constexpr size_t bytes = PipePlan<NQ, TQ, TV, TC, STAGE>::BYTES;
-  return bytes <= kPipeMaxSmem && bytes <= device_smem_optin();
+  int r = (bytes <= kPipeMaxSmem && bytes <= optin) ? 1 : 0;
+  if constexpr (NQ >= 9) {
+    constexpr size_t sb = SplitPlan<NQ, kSplitH<NQ>, TQ, TV, TC, STAGE>::BYTES;
+    if (sb <= kPipeMaxSmem && sb <= optin) r |= 2;
+  }
+  return r;
 }
 
 // Pipelined-kernel facts for this order: elements per tile, and whether the

@@ -1,0 +1,448 @@
+// Split-column variant of the persistent fused kernel, for the high orders
+// (one element per tile, Nq >= 9).
+//
+// In tend_pipe_kernel one element is handled by Nq^2 threads, each owning a
+// whole z-column of Nq nodes.  From Nq = 9 on a tile is one element, and the
+// element's shared-memory ring allows one to three blocks per SM, so an SM
+// holds only 5-7 warps: too few to cover the latency of the column loads,
+// line contractions and face gathers.  Here each column is split over H
+// threads, H = 2 (thread T = c + Nq^2 h owns nodes k in [h*KZ, (h+1)*KZ) of
+// column c, KZ = ceil(Nq/H)), so a tile has H*Nq^2 threads, each with half
+// the column's registers, and the other phases are shared out by h:
+//
+//   phase 1   every thread: its nodes' volume fluxes, q*w in place of w,
+//             minus-side face values;
+//   lines     h = 0 contracts x-line c, h = 1 y-line c;
+//   faces     h = 0: the two y faces at face node c and the -z face of
+//             column c (it owns node k = 0); h = 1: the two x faces and
+//             the +z face (it owns node k = Nq-1);
+//   epilogue  every thread: z-derivative (from the whole q*w column in
+//             shared memory), lift, combine and RK stage of its nodes.
+//
+// Every node goes through exactly the operations, operands and order of
+// tend_pipe_kernel and tend_kernel, so all variants compute identical bits.
+// The ring (cp.async.bulk of q, u, v, w, escale and fscale into NSTAGE
+// slots, bounded mbarrier waits, status word on a timeout) is the one of
+// tend_pipe_kernel with one element per tile.
+#pragma once
+
+#include "sdg_tend_pipe.cuh"
+
+namespace sdg {
+
+template <int NQ, int H>
+struct SplitGeo {
+  static constexpr int NQ2 = NQ * NQ;
+  static constexpr int NP = NQ2 * NQ;
+  static constexpr int THREADS = H * NQ2;
+  static constexpr int KZ = (NQ + H - 1) / H;  // column nodes per thread
+};
+
+// Shared-memory plan: the ring of one-element slots, the minus-side face
+// values (FaceArea), the face fluxes ((f1, f3) and (f2, f4) pairs per face
+// node, f5 and f6 per column), the factored lift's x/y factors, barriers.
+template <int NQ, int H, typename TQ, typename TV, typename TC, bool STAGE>
+struct SplitPlan {
+  static constexpr int NQ2 = NQ * NQ;
+  static constexpr int NP = NQ2 * NQ;
+  static constexpr int NSTAGE = 2;
+  static constexpr size_t r16(size_t x) { return (x + 15) & ~size_t(15); }
+  static constexpr size_t mx(size_t a, size_t b) { return a > b ? a : b; }
+  static constexpr size_t QB = r16(sizeof(TQ) * NP + 32);
+  static constexpr size_t VB =
+      mx(r16(sizeof(TV) * NP + 32),
+         r16(sizeof(TC) * LineIdx<NQ, static_cast<int>(sizeof(TC))>::SIZE));
+  static constexpr size_t EB = r16(sizeof(TC) * 3 + 32);
+  static constexpr size_t FB = r16(sizeof(TC) * 6 + 32);
+  static constexpr size_t OFF_U = QB;
+  static constexpr size_t OFF_V = QB + VB;
+  static constexpr size_t OFF_W = QB + 2 * VB;
+  static constexpr size_t OFF_E = QB + 3 * VB;
+  static constexpr size_t OFF_F = OFF_E + EB;
+  static constexpr size_t SLOT = OFF_F + FB;
+  static constexpr size_t FACE = r16(sizeof(TC) * FaceArea<NQ, sizeof(TC) == 8>::ELEM);
+  static constexpr size_t FLUX = r16(sizeof(TC) * 6 * NQ2);
+  static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
+  static constexpr size_t BARS = 16 * NSTAGE;
+  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + FLUX + LIFTB + BARS;
+  static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
+      kSmemPerSM / (BYTES + kSmemPerBlockReserved) > 4
+          ? 4
+          : (kSmemPerSM / (BYTES + kSmemPerBlockReserved) < 1
+                 ? 1
+                 : kSmemPerSM / (BYTES + kSmemPerBlockReserved)));
+};
+
+// Columns split in two from Nq = 9 on.
+template <int NQ>
+constexpr int kSplitH = 2;
+
+// Blocks per SM the kernel is built for: what the shared memory allows,
+// capped so that a thread keeps at least 128 (FP64) or 80 (FP32) registers.
+template <int NQ, int H, typename TQ, typename TV, typename TC, bool STAGE>
+constexpr int split_min_blocks() {
+  constexpr int m = SplitPlan<NQ, H, TQ, TV, TC, STAGE>::BLOCKS_PER_SM_SMEM;
+  constexpr int thr = (SplitGeo<NQ, H>::THREADS + 31) / 32 * 32;
+  constexpr int floor_regs = sizeof(TC) == 8 ? 128 : 80;
+  constexpr int by_regs = 65536 / (thr * floor_regs);
+  constexpr int r = m < by_regs ? m : by_regs;
+  return r < 1 ? 1 : r;
+}
+
+template <int NQ, int H, typename TQ, typename TV, typename TO, typename TC, bool EXACT,
+          int ORDER, bool STAGE, bool BATCH>
+__global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
+                                  (split_min_blocks<NQ, H, TQ, TV, TC, STAGE>()))
+    tend_split_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
+                      const __grid_constant__ DMat<NQ, TC> D) {
+  using G = SplitGeo<NQ, H>;
+  using P = SplitPlan<NQ, H, TQ, TV, TC, STAGE>;
+  using AR = Ar<TC, EXACT>;
+  using Ctx = TileCtx<TQ, TV, TO, TC>;
+  using V2 = typename Pair2<TC>::type;
+  using LI = LineIdx<NQ, static_cast<int>(sizeof(TC))>;
+  constexpr int NQ2 = G::NQ2;
+  constexpr int NP = G::NP;
+  constexpr int KZ = G::KZ;
+  constexpr int NS = P::NSTAGE;
+  static_assert(H == 2, "columns split in two parts");
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* slots = smem_raw;
+  TC* fa = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT);
+  TC* flux = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::FACE);
+  TC* sL = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::FACE + P::FLUX);
+  uint64_t* bars =
+      reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::FACE + P::FLUX + P::LIFTB);
+
+  const int h = threadIdx.x / NQ2;      // part of the column
+  const int c = threadIdx.x - h * NQ2;  // column a + NQ*b
+  const int a = c % NQ;
+  const int b = c / NQ;
+  const int k0 = h * KZ;                // first node of this thread's part
+  const int ntiles = BATCH ? A.ntiles : A.nelem;
+  const bool own_y = h == 0;            // y faces and the -z face
+  const bool own_x = h == H - 1;        // x faces and the +z face
+  const unsigned spins = A.wait_spins;
+
+  // Minus-side face values (FaceArea): FP64 keeps the x faces in two scalar
+  // arrays and the y faces as (q, v) pairs; FP32 keeps (q, un) pairs of the
+  // four faces, face-major.
+  constexpr bool XSPLIT = sizeof(TC) == 8;
+  using FA = FaceArea<NQ, XSPLIT>;
+  TC* xq = fa;
+  TC* xu = fa + FA::XA;
+  V2* ypair = reinterpret_cast<V2*>(fa + FA::Y0);
+  V2* fM = reinterpret_cast<V2*>(fa);
+  // Face fluxes: (f1, f3) and (f2, f4) at face node n, f5 and f6 at column n.
+  V2* fl13 = reinterpret_cast<V2*>(flux);
+  V2* fl24 = fl13 + NQ2;
+  TC* fl5 = flux + 4 * NQ2;
+  TC* fl6 = flux + 5 * NQ2;
+
+  // Producer: one thread fills ring slot `slot` with tile (element) `tile`.
+  auto issue = [&](int tile, int slot) {
+    // Test hook (host-set): leave this tile's slot empty.
+    if (tile + 1 == A.inject_skip) return;
+    const Ctx cx = tile_ctx<1, BATCH>(A, tile, ntiles);
+    unsigned char* base = slots + slot * P::SLOT;
+    const void* src[6] = {cx.q, cx.u, cx.v, cx.w, cx.escale, cx.fscale};
+    const size_t per[6] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
+                           sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6};
+    const size_t off[6] = {0, P::OFF_U, P::OFF_V, P::OFF_W, P::OFF_E, P::OFF_F};
+    size_t lo[6];
+    uint32_t by[6], sh[6], total = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      tile_range(cx.e0, cx.n, per[k], &lo[k], &by[k], &sh[k]);
+      total += by[k];
+    }
+    mbar_arrive_expect_tx(&bars[slot], total);
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
+               &bars[slot]);
+    if (STAGE && A.rk_a != 0.0) {
+      size_t l0;
+      uint32_t b0, s0;
+      tile_range(cx.e0, cx.n, sizeof(double) * NP, &l0, &b0, &s0);
+      bulk_prefetch_l2(reinterpret_cast<const unsigned char*>(cx.q0) + l0, b0);
+    }
+  };
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NS; ++k) mbar_init(&bars[k], 1);
+    fence_barrier_init();
+  }
+  if constexpr (!EXACT) {
+    for (int x = threadIdx.x; x < 4 * NQ; x += blockDim.x) {
+      const int f = x / NQ, n = x - f * NQ;
+      sL[x] = ldro(A.lift + NP * f + ((f & 1) ? n : NQ * n));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NS; ++k) {
+      const int tile = blockIdx.x + k * gridDim.x;
+      if (tile < ntiles) issue(tile, k);
+    }
+
+  for (int it = 0;; ++it) {
+    const int tile = blockIdx.x + it * gridDim.x;
+    if (tile >= ntiles) break;
+    const int slot = it % NS;
+    const uint32_t parity = (it / NS) & 1;
+    const Ctx C = tile_ctx<1, BATCH>(A, tile, ntiles);
+    const int e = C.e0;
+    const long base = static_cast<long>(e) * NP;
+
+    // The faces this thread evaluates: their neighbour rows, needed after
+    // phase 1.
+    int pbc[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const bool mine = (f == 0 || f == 2 || f == 4) ? own_y : own_x;
+      pbc[f] = mine ? ldro(C.pbase + 6 * static_cast<long>(e) + f) : 0;
+    }
+
+    // ---- Wait for the tile's slot (bounded, block-uniform) ---------------
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity, spins));
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        atomicExch(A.status, kStatusWaitTimeout);
+        for (int k = 0; k < NS; ++k) {
+          const int T = it + k;
+          const int tk = blockIdx.x + T * gridDim.x;
+          if (tk < ntiles && (T < NS || T - NS + 1 <= it - 1))
+            mbar_wait_bounded(&bars[T % NS], (T / NS) & 1, spins);
+        }
+      }
+      return;
+    }
+    if (threadIdx.x == 0 && it > 0) {
+      const int nt = blockIdx.x + (it - 1 + NS) * gridDim.x;
+      if (nt < ntiles) issue(nt, (it - 1) % NS);
+    }
+
+    unsigned char* sb = slots + slot * P::SLOT;
+    const TQ* sq = reinterpret_cast<const TQ*>(sb + tile_shift(C.e0, sizeof(TQ) * NP));
+    const uint32_t shv = tile_shift(C.e0, sizeof(TV) * NP);
+    const TV* su = reinterpret_cast<const TV*>(sb + P::OFF_U + shv);
+    const TV* sv = reinterpret_cast<const TV*>(sb + P::OFF_V + shv);
+    const TV* sw = reinterpret_cast<const TV*>(sb + P::OFF_W + shv);
+    const TC* ses = reinterpret_cast<const TC*>(sb + P::OFF_E + tile_shift(C.e0, sizeof(TC) * 3));
+    const TC* sfs = reinterpret_cast<const TC*>(sb + P::OFF_F + tile_shift(C.e0, sizeof(TC) * 6));
+    static_assert(sizeof(TV) == sizeof(TC), "w and q*w share their slots");
+    TC* sz = reinterpret_cast<TC*>(sb + P::OFF_W + shv);
+    TC* sX = reinterpret_cast<TC*>(sb + P::OFF_U);
+    TC* sY = reinterpret_cast<TC*>(sb + P::OFF_V);
+
+    // ---- Plus-side face values, from global memory (L2) -------------------
+    // Slots 0, 1: the two x or y faces of this thread; 2: its z face.
+    TC qP[3], unP[3];
+    auto gather = [&]() {
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        const bool mine = (f == 0 || f == 2 || f == 4) ? own_y : own_x;
+        if (!mine) continue;
+        // slot of face f among this thread's faces
+        const int sl = (f >= 4) ? 2 : ((f == 0 || f == 1) ? 0 : 1);
+        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
+                                       : static_cast<long>(-1 - pbc[f]) + c;
+        qP[sl] = static_cast<TC>(ldro(C.q + idx));
+        unP[sl] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx)
+                                                     : ((f >= 4) ? ldro(C.w + idx)
+                                                                 : ldro(C.v + idx)));
+      }
+    };
+    constexpr bool EARLY = sizeof(TC) == 8;
+    if constexpr (EARLY) gather();
+
+    // ---- Phase 1: this thread's nodes of column c -------------------------
+    TC fx[KZ], fy[KZ];
+    TC wlo = TC(0), whi = TC(0), qlo = TC(0), qhi = TC(0);
+    {
+      const bool onx = (a == 0) || (a == NQ - 1);
+      const bool ony = (b == 0) || (b == NQ - 1);
+      const int xo = (a == 0 ? FA::XOFF : 0) + b;
+      V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
+      V2* fmy = XSPLIT ? ypair + (b == 0 ? 0 : NQ2) + a : fM + (b == 0 ? 0 : 2) * NQ2 + a;
+#pragma unroll
+      for (int kk = 0; kk < KZ; ++kk) {
+        const int k = k0 + kk;
+        if (KZ * H != NQ && k >= NQ) break;
+        const int n = c + NQ2 * k;
+        const TC qv = static_cast<TC>(sq[n]);
+        const TC uv = static_cast<TC>(su[n]);
+        const TC vv = static_cast<TC>(sv[n]);
+        const TC wv = static_cast<TC>(sw[n]);
+        if (k == 0) {
+          wlo = wv;
+          qlo = qv;
+        }
+        if (k == NQ - 1) {
+          whi = wv;
+          qhi = qv;
+        }
+        fx[kk] = AR::mul(qv, uv);
+        fy[kk] = AR::mul(qv, vv);
+        sz[n] = AR::mul(qv, wv);
+        if constexpr (XSPLIT) {
+          if (onx) {
+            xq[xo + NQ * k] = qv;
+            xu[xo + NQ * k] = uv;
+          }
+        } else {
+          if (onx) fmx[NQ * k] = V2{qv, uv};
+        }
+        if (ony) fmy[NQ * k] = V2{qv, vv};
+      }
+    }
+    __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
+#pragma unroll
+    for (int kk = 0; kk < KZ; ++kk) {
+      const int k = k0 + kk;
+      if (KZ * H != NQ && k >= NQ) break;
+      sX[LI::colx(a, b, k)] = fx[kk];
+      sY[LI::coly(a, b, k)] = fy[kk];
+    }
+    __syncthreads();
+    if constexpr (!EARLY) gather();
+
+    double q0r[STAGE ? KZ : 1];
+    const bool use_q0 = STAGE && A.rk_a != 0.0;
+    // ---- Lines: x-line c (h = 0) and y-line c (h = 1), in place ----------
+    {
+      const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
+      if (h == 0) {
+        TC line[NQ];
+#pragma unroll
+        for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i)
+          sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
+              [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
+      }
+      if (h == H - 1) {
+        TC line[NQ];
+#pragma unroll
+        for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
+#pragma unroll
+        for (int j = 0; j < NQ; ++j)
+          sY[LI::yl(lby, j)] = contract<NQ, ORDER, AR, TC>(
+              [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
+      }
+    }
+    // The line buffers live in the slot that the next refill overwrites.
+    fence_proxy_async_smem();
+    if constexpr (STAGE) {
+      if (use_q0) {
+#pragma unroll
+        for (int kk = 0; kk < KZ; ++kk) {
+          const int k = k0 + kk;
+          if (KZ * H != NQ && k >= NQ) break;
+          q0r[kk] = ld_stream(C.q0 + base + c + NQ2 * k);
+        }
+      }
+    }
+    // ---- Face fluxes ------------------------------------------------------
+    if (own_y) {
+      // y faces at face node c: -y (1) and +y (3); -z (5) of column c.
+      V2 m1, m3;
+      if constexpr (XSPLIT) {
+        m1 = ypair[c];
+        m3 = ypair[NQ2 + c];
+      } else {
+        m1 = fM[c];
+        m3 = fM[2 * NQ2 + c];
+      }
+      const TC f1 = upwind_flux<AR, TC>(m1.x, m1.y, qP[0], unP[0], TC(-1), sfs[0]);
+      const TC f3 = upwind_flux<AR, TC>(m3.x, m3.y, qP[1], unP[1], TC(1), sfs[2]);
+      fl13[c] = V2{f1, f3};
+      fl5[c] = upwind_flux<AR, TC>(qlo, wlo, qP[2], unP[2], TC(-1), sfs[4]);
+    }
+    if (own_x) {
+      // x faces at face node c: +x (2) and -x (4); +z (6) of column c.
+      TC q2, u2, q4, u4;
+      if constexpr (XSPLIT) {
+        const int xn = NQ * b + a;
+        q2 = xq[xn];
+        u2 = xu[xn];
+        q4 = xq[FA::XOFF + xn];
+        u4 = xu[FA::XOFF + xn];
+      } else {
+        const V2 m2 = fM[NQ2 + c], m4 = fM[3 * NQ2 + c];
+        q2 = m2.x;
+        u2 = m2.y;
+        q4 = m4.x;
+        u4 = m4.y;
+      }
+      const TC f2 = upwind_flux<AR, TC>(q2, u2, qP[0], unP[0], TC(1), sfs[1]);
+      const TC f4 = upwind_flux<AR, TC>(q4, u4, qP[1], unP[1], TC(-1), sfs[3]);
+      fl24[c] = V2{f2, f4};
+      fl6[c] = upwind_flux<AR, TC>(qhi, whi, qP[2], unP[2], TC(1), sfs[5]);
+    }
+    __syncthreads();
+
+    // ---- Epilogue: z-derivative, lift, combine, store ---------------------
+    {
+      const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
+      TC lxy[4];
+      if constexpr (!EXACT) {
+        lxy[0] = sL[b];
+        lxy[1] = sL[NQ + a];
+        lxy[2] = sL[2 * NQ + b];
+        lxy[3] = sL[3 * NQ + a];
+      }
+      const TC f5 = fl5[c], f6 = fl6[c];
+      TC fz[NQ];
+#pragma unroll
+      for (int l = 0; l < NQ; ++l) fz[l] = sz[c + NQ2 * l];
+#pragma unroll
+      for (int kk = 0; kk < KZ; ++kk) {
+        const int k = k0 + kk;
+        if (KZ * H != NQ && k >= NQ) break;
+        const TC dz = contract<NQ, ORDER, AR, TC>([&](int l) { return fz[l]; },
+                                                  [&](int l) { return D.d[k * NQ + l]; });
+        TC L[6];
+        if constexpr (!EXACT) {
+#pragma unroll
+          for (int f = 0; f < 4; ++f) L[f] = lxy[f];
+          L[4] = D.lz[k];
+          L[5] = D.lz[NQ + k];
+        } else {
+#pragma unroll
+          for (int f = 0; f < 6; ++f) L[f] = ldro(A.lift + c + NQ2 * k + NP * f);
+        }
+        // tensorprod_Lift_hexahedral (kern:278-283), face order 1..6.
+        const V2 f13 = fl13[a + NQ * k];
+        const V2 f24 = fl24[b + NQ * k];
+        TC lf = AR::mul(L[0], f13.x);
+        lf = AR::mad(L[1], f24.x, lf);
+        lf = AR::mad(L[2], f13.y, lf);
+        lf = AR::mad(L[3], f24.y, lf);
+        lf = AR::mad(L[4], f5, lf);
+        lf = AR::mad(L[5], f6, lf);
+        // dqdt = -(Escale1*DxF + Escale2*DyF + Escale3*DzF + Lift), eq:194-198.
+        TC acc = AR::mul(e1, sX[LI::colx(a, b, k)]);
+        acc = AR::mad(e2, sY[LI::coly(a, b, k)], acc);
+        acc = AR::mad(e3, dz, acc);
+        acc = AR::add(acc, lf);
+        const TC dqdt = -acc;
+        const long n = base + c + NQ2 * k;
+        if constexpr (!STAGE) {
+          C.out[n] = static_cast<TO>(dqdt);
+        } else {
+          // q = rk_a*q0 + rk_b*(q + dt*dqdt), main.f90:70-71, in FP64.
+          using AD = Ar<double, EXACT>;
+          const double qd = static_cast<double>(sq[c + NQ2 * k]);
+          double r = AD::mul(A.rk_b, AD::mad(C.dt, static_cast<double>(dqdt), qd));
+          if (use_q0) r = AD::mad(A.rk_a, q0r[kk], r);
+          C.out[n] = static_cast<TO>(r);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace sdg

@@ -41,10 +41,12 @@ SDG_ERR_STATE = 5
 FLAG_EXACT = 1
 FLAG_ORDER_GENERAL = 2
 FLAG_MIXED = 4
+FLAG_EXTERNAL_HALO = 8
 
 FIELD_Q, FIELD_U, FIELD_V, FIELD_W = 0, 1, 2, 3
+ARRAY_STAGE2, ARRAY_STAGE3 = 4, 5
 
-VARIANT_AUTO, VARIANT_BLOCK, VARIANT_PIPE = 0, 1, 2
+VARIANT_AUTO, VARIANT_BLOCK, VARIANT_PIPE, VARIANT_BLOCK8, VARIANT_SPLIT = 0, 1, 2, 3, 4
 
 # Exported symbols and their signatures (must match include/sdg_gpu.h).
 _I, _D, _P, _LL = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
@@ -75,6 +77,8 @@ SIGNATURES = {
     "sdg_get_stream": (_I, [_P, ctypes.POINTER(_P)]),
     "sdg_field_dev_ptr": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "sdg_timers": (_I, [_P, _P]),
+    "sdg_resident_array": (_I, [_P, _I, ctypes.POINTER(_P), ctypes.POINTER(_I)]),
+    "sdg_update_halo_stage": (_I, [_P, _I]),
     "sdg_launch_count": (_LL, [_P]),
     "sdg_set_kernel_variant": (_I, [_P, _I]),
     "sdg_debug_inject_wait_timeout": (_I, [_P, _I, _I]),
@@ -357,6 +361,23 @@ class Handle:
         _check(lib().sdg_field_dev_ptr(self._h, which, ctypes.byref(p)))
         return p.value
 
+    def resident_array(self, which):
+        """A resident (Np, NeA) device array as a flat torch tensor view (no
+        copy): FIELD_Q, FIELD_U/V/W (compute precision) or ARRAY_STAGE2/3."""
+        import torch
+        p, es = ctypes.c_void_p(), ctypes.c_int()
+        _check(lib().sdg_resident_array(self._h, which, ctypes.byref(p), ctypes.byref(es)))
+        n = self.mesh.Np * self.mesh.NeA
+        return _device_view(p.value, n, torch.float64 if es.value == 8 else torch.float32)
+
+    def stage_input(self, stage):
+        """The input array of RK stage 1..3 (see resident_array)."""
+        return self.resident_array((FIELD_Q, ARRAY_STAGE2, ARRAY_STAGE3)[stage - 1])
+
+    def update_halo_stage(self, stage):
+        """update_halo of stage `stage`'s input on the handle's stream."""
+        _check(lib().sdg_update_halo_stage(self._h, stage))
+
     def timers(self):
         t = np.zeros(4)
         _check(lib().sdg_timers(self._h, _p(t)))
@@ -366,7 +387,9 @@ class Handle:
         return int(lib().sdg_launch_count(self._h))
 
     def set_kernel_variant(self, variant):
-        """0 automatic, 1 one tile per block, 2 persistent bulk-copy ring."""
+        """0 automatic, 1 one tile per block, 2 persistent bulk-copy ring,
+        3 one tile per block at 8 blocks per SM, 4 bulk-copy ring with split
+        columns (orders with one element per tile)."""
         _check(lib().sdg_set_kernel_variant(self._h, variant))
 
     def inject_wait_timeout(self, tile, spins=0):
@@ -374,6 +397,21 @@ class Handle:
         `tile`, so its bounded wait runs out after `spins` polls and the next
         synchronising call raises; tile < 0 turns it off."""
         _check(lib().sdg_debug_inject_wait_timeout(self._h, tile, spins))
+
+
+def _device_view(ptr, n, dtype):
+    """A torch tensor over n elements of device memory at ptr (no copy,
+    not owned: the library keeps the allocation)."""
+    import torch
+
+    class _Arr:
+        pass
+
+    a = _Arr()
+    a.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8" if dtype == torch.float64
+                                  else "<f4", "data": (ptr, False), "version": 3,
+                                  "strides": None}
+    return torch.as_tensor(a, device="cuda")
 
 
 # ---------------------------------------------------------------------------
@@ -502,10 +540,10 @@ class Batch:
         v = buf[:n]
         groups = []
         for g in range(int(v[4])):
-            r = v[5 + 7 * g: 12 + 7 * g]
+            r = v[5 + 8 * g: 13 + 8 * g]
             groups.append({"p": int(r[0]), "mixed": bool(r[1]), "tiles": int(r[2]),
                            "variant": int(r[3]), "ms_pipe": r[4], "ms_block": r[5],
-                           "ms_block8": r[6]})
+                           "ms_block8": r[6], "ms_split": r[7]})
         return {"instances": int(v[0]), "dof": int(v[1]), "run_s": v[2],
                 "dof_steps": int(v[3]), "groups": groups}
 

@@ -33,13 +33,16 @@ def _case(p, dims, seed=3):
     return ops, mesh, fields
 
 
-@pytest.mark.parametrize("flags", [0, sdg.FLAG_EXACT, sdg.FLAG_MIXED])
-def test_rk_wait_timeout_is_reported_and_handle_recovers(flags):
-    p, dims = 7, (4, 4, 4)           # 64 elements, 32 tiles of two
+@pytest.mark.parametrize("flags,p,variant",
+                         [(0, 7, sdg.VARIANT_PIPE), (sdg.FLAG_EXACT, 7, sdg.VARIANT_PIPE),
+                          (sdg.FLAG_MIXED, 7, sdg.VARIANT_PIPE), (0, 9, sdg.VARIANT_SPLIT),
+                          (sdg.FLAG_MIXED, 11, sdg.VARIANT_SPLIT)])
+def test_rk_wait_timeout_is_reported_and_handle_recovers(flags, p, variant):
+    dims = (4, 4, 4) if p <= 7 else (3, 3, 3)  # 32 tiles of two, or 27 of one
     ops, mesh, (q, u, v, w) = _case(p, dims)
-    dt = 0.1 / 4 / (p + 1) ** 2
+    dt = 0.1 / dims[0] / (p + 1) ** 2
     H = sdg.Handle(ops, mesh, flags)
-    H.set_kernel_variant(sdg.VARIANT_PIPE)
+    H.set_kernel_variant(variant)
     H.set_state(q, u, v, w)
     H.inject_wait_timeout(5, spins=4096)
     H.rk3_steps(dt, 1)               # asynchronous: the error surfaces at sync
@@ -55,6 +58,7 @@ def test_rk_wait_timeout_is_reported_and_handle_recovers(flags):
     got = H.get_field()
     H.close()
     H2 = sdg.Handle(ops, mesh, flags)
+    H2.set_kernel_variant(sdg.VARIANT_BLOCK)
     H2.set_state(q, u, v, w)
     H2.rk3_steps(dt, 3)
     ref = H2.get_field()

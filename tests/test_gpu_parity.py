@@ -191,7 +191,7 @@ def test_full_size_rhs_against_oracle():
     assert rel_maxnorm(got, ref) <= TOL
 
 
-@pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE])
+@pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE, sdg.VARIANT_SPLIT])
 @pytest.mark.parametrize("p", range(1, 16))
 def test_kernel_variants_bitwise(p, variant):
     """Both kernel variants (one tile per block; persistent bulk-copy ring)
@@ -212,8 +212,8 @@ def test_kernel_variants_bitwise(p, variant):
     h.close()
 
 
-@pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE])
-@pytest.mark.parametrize("p", [3, 4, 5, 6, 7, 10, 12, 13, 15])
+@pytest.mark.parametrize("variant", [sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE, sdg.VARIANT_SPLIT])
+@pytest.mark.parametrize("p", [3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15])
 def test_mixed_variants_agree(p, variant):
     """Mixed form: the pipelined kernel (packed FP32 line contractions at
     p = 3, 7, 10-15, its own FP32 line layouts at p = 5-7) and the
@@ -244,16 +244,17 @@ def test_partial_last_tile_and_uneven_sizes():
         h.close()
 
 
-@pytest.mark.parametrize("p", [11, 12, 13, 14, 15])
+@pytest.mark.parametrize("p", [8, 9, 10, 11, 12, 13, 14, 15])
 def test_fast_high_order_variants_agree(p):
-    """Fast FP64 at p = 11-15: the pipelined kernel at one block per SM (up
-    to the 227 KB plan of p = 14) and the one-tile-per-block kernel give the
-    same bits over RK steps, and both stay within 1e-12 of the oracle."""
+    """Fast FP64 at p = 8-15: the pipelined kernel (one block per SM from
+    p = 11, up to the 227 KB plan of p = 14), the split-column kernel and the
+    one-tile-per-block kernel give the same bits over RK steps, and stay
+    within 1e-12 of the oracle."""
     dims, nstep = (2, 3, 2), 3
     ops, mesh, omesh, (q, u, v, w) = case(p, dims)
     dt = 0.1 / 3 / (p + 1) ** 2
     res = []
-    for var in (sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE):
+    for var in (sdg.VARIANT_BLOCK, sdg.VARIANT_PIPE, sdg.VARIANT_SPLIT):
         h = sdg.Handle(ops, mesh, 0)
         h.set_kernel_variant(var)
         h.set_state(q, u, v, w)
@@ -261,6 +262,7 @@ def test_fast_high_order_variants_agree(p):
         res.append(h.get_field())
         h.close()
     assert np.array_equal(res[0], res[1])
+    assert np.array_equal(res[0], res[2])
     qo = q.copy(order="F")
     orc.run_rk3(orc.OPT1, qo, u, v, w, ops, omesh, dt, nstep)
     assert rel_maxnorm(res[1], qo[:, : mesh.Ne]) <= TOL
