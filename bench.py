@@ -87,6 +87,8 @@ def parse(argv=None):
     ap.add_argument("--seq-sample", type=int, default=100,
                     help="served workload: requests solved one at a time (plain FP64) "
                          "for comparison")
+    ap.add_argument("--orders", default="1-15",
+                    help="pscan: the orders to sweep, e.g. 1-15 or 8,9,11")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0,
                     help="budget of the CPU-baseline sample")
@@ -482,66 +484,115 @@ def time_batch(sdg, rep, mixed, steps, warmup, gidx, bf):
 
 
 def time_served(sdg, rep, nreq, seq_sample, gidx):
-    """Poisson request stream at ~80 % load against the serving loop; the
-    arrival rate comes from one-at-a-time FP64 solves of the first requests."""
+    """Poisson request stream at ~80 % load against the serving loop.  The
+    arrival rate comes from one-at-a-time plain FP64 solves (each request
+    alone on the GPU, CUDA-graph steps) of the first `seq_sample` requests.
+    Each request's fields are generated ahead of its arrival by a producer
+    thread (bounded look-ahead), and results are fetched as they complete,
+    so the host holds only the requests in flight."""
+    import queue
     reqs, rng = served_stream(nreq)
     ops = {p: sdg.read_operators(p) for p in range(3, 12)}
-    fields = []
-    for r in reqs:
+
+    def make_fields(r):
         vel = tuple(sdg.random_velocity(r["seed"]))
-        fields.append(sdg.box_fields(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D,
-                                     ic_kind=1, seed=r["seed"], vel_kind=0, vel=vel))
-    work = [r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"] for r in reqs]
+        return sdg.box_fields(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D,
+                              ic_kind=1, seed=r["seed"], vel_kind=0, vel=vel)
+
+    def dof(r):
+        return r["ne"] ** 3 * (r["p"] + 1) ** 3
+
+    work = [dof(r) * 3 * r["nstep"] for r in reqs]
+    # One at a time, plain FP64: each request alone in a one-instance batch.
     n_seq = min(len(reqs), seq_sample)
     t_seq, w_seq = 0.0, 0
-    for r, f in zip(reqs[:n_seq], fields[:n_seq]):
-        m = sdg.mesh_setup(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]].x1D)
-        h = sdg.Handle(ops[r["p"]], m, 0)
-        full = [np.zeros((m.Np, m.NeA), order="F") for _ in range(4)]
-        n = m.Np * m.Ne
-        for dst, src in zip(full, f):
-            dst.reshape(-1, order="F")[:n] = src.reshape(-1, order="F")[:n]
-        h.set_state(*full)
-        h.synchronize()
-        t0 = time.perf_counter()
-        h.rk3_steps(r["dt"], r["nstep"])
-        h.synchronize()
-        t_seq += time.perf_counter() - t0
-        w_seq += r["ne"] ** 3 * (r["p"] + 1) ** 3 * 3 * r["nstep"]
-        h.close()
-        del m, full
+    for r in reqs[:n_seq]:
+        f = make_fields(r)
+        b = sdg.Batch(0)
+        b.add(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]], *f, r["dt"])
+        del f
+        b.commit(autotune=False)
+        b.run(1)
+        i0 = b.info()["run_s"]
+        b.run(r["nstep"])
+        t_seq += b.info()["run_s"] - i0
+        w_seq += dof(r) * 3 * r["nstep"]
+        b.close()
     seq_rate = w_seq / t_seq
     lam = 0.8 * seq_rate / float(np.mean(work))   # requests per second at ~80 % load
     gaps = rng.exponential(1.0 / lam, size=len(reqs))
+
+    ahead = queue.Queue(maxsize=24)
+
+    def producer():
+        for r in reqs:
+            ahead.put((r, make_fields(r)))
+
     srv = sdg.Server()
+    ids, late, tts, qwait = [], 0, [], []
+    pending = {}
+    lock = threading.Lock()
+    stop = threading.Event()
+
+    def collect(final=False):
+        with lock:
+            items = list(pending.items())
+        for i, shape in items:
+            st, qw, t = srv.poll(i)
+            if st == sdg.SERVE_DONE:
+                srv.result(i)
+                with lock:
+                    del pending[i]
+                tts.append(t)
+                qwait.append(qw)
+            elif st == sdg.SERVE_FAILED:
+                raise RuntimeError(f"served request {i} failed")
+
+    def collector():
+        while not stop.is_set():
+            collect()
+            time.sleep(0.005)
+
+    threading.Thread(target=producer, daemon=True).start()
     with ClockSampler(gidx) as clk:
         rep.barrier()
+        col = threading.Thread(target=collector, daemon=True)
+        col.start()
         t_start = time.perf_counter()
-        ids = []
         t_next = t_start
-        for r, f, g in zip(reqs, fields, gaps):
+        for g in gaps:
+            r, f = ahead.get()
             t_next += g
             d = t_next - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            ids.append(srv.submit(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]], *f,
-                                  r["dt"], r["nstep"], mixed=r["mixed"]))
+            elif d < -0.01:
+                late += 1
+            i = srv.submit(r["ne"], r["ne"], r["ne"], r["p"], ops[r["p"]], *f, r["dt"],
+                           r["nstep"], mixed=r["mixed"])
+            del f
+            with lock:
+                pending[i] = True
+            ids.append(i)
+        t_arrivals = time.perf_counter() - t_start
         srv.wait(0)
         makespan = time.perf_counter() - t_start
-    polls = [srv.poll(i) for i in ids]
-    tts = np.array([p[2] for p in polls])
-    qwait = np.array([p[1] for p in polls])
+        stop.set()
+        col.join()
+    collect(final=True)
     st = srv.stats()
     srv.close()
+    tts = np.array(tts)
+    qwait = np.array(qwait)
     total = float(sum(work))
     value = rep.rate(total, makespan)
     makespan = rep.max(makespan)
     busy = rep.max(st["busy_s"])
     busy_rate = rep.sum(st["dof_steps"] * 3) / max(busy, 1e-9)
-    bytes_step = sum(r["ne"] ** 3 * (r["p"] + 1) ** 3 * r["nstep"] *
-                     sum(stage_bytes_per_dof(r["mixed"])) for r in reqs)
+    bytes_step = sum(dof(r) * r["nstep"] * sum(stage_bytes_per_dof(r["mixed"])) for r in reqs)
     peak, peak_kind = measured_peaks()
     achieved = rep.sum(bytes_step) / max(busy, 1e-9) / 1e9
+    seq_all = rep.sum(seq_rate)
     return {"value": value, "unit": METRIC, "ms_per_step": 1e3 * makespan / len(reqs),
             "steps": len(reqs), "warmup": 0, "dtype": "f32+f64",
             "config": {"workload": "served", "requests": len(reqs),
@@ -553,12 +604,13 @@ def time_served(sdg, rep, nreq, seq_sample, gidx):
                        "mean_tts_s": float(tts.mean()),
                        "p50_queue_s": float(np.percentile(qwait, 50)),
                        "p99_queue_s": float(np.percentile(qwait, 99)),
-                       "makespan_s": makespan, "device_busy_s": busy,
+                       "makespan_s": makespan, "arrivals_s": t_arrivals,
+                       "late_arrivals": late, "device_busy_s": busy,
                        "throughput_busy": busy_rate,
-                       "one_at_a_time_fp64": rep.sum(seq_rate),
-                       "busy_vs_one_at_a_time": busy_rate / rep.sum(seq_rate),
+                       "one_at_a_time_fp64": seq_all,
+                       "busy_vs_one_at_a_time": busy_rate / seq_all,
                        "one_at_a_time_sample": n_seq,
-                       "iterations": st["iterations"]},
+                       "rk_steps_run": st["iterations"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                          "over": "device-busy time",
@@ -808,9 +860,13 @@ def run_pscan(args):
     import sdg_b200 as sdg
     peak, peak_kind = measured_peaks()
     names = {1: "Block", 2: "Pipe", 3: "BlockOcc", 4: "Split"}
+    orders = []
+    for part in args.orders.split(","):
+        lo, _, hi = part.partition("-")
+        orders += list(range(int(lo), int(hi or lo) + 1))
     rows = []
     for mixed in (False, True):
-        for p in range(1, 16):
+        for p in orders:
             nq = p + 1
             N = max(2, round((16.8e6 / nq ** 3) ** (1 / 3)))
             ops = sdg.read_operators(p)

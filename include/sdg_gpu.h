@@ -121,6 +121,15 @@ int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
                     int Np, int Ne, double* q, double* u, double* v,
                     double* w);
 
+/* sdg_init_fields on the periodic unit box NeX x NeY x NeZ of order p
+ * without the mesh tables: the node positions of sdg_mesh_setup are formed
+ * where they are used (the same values bit for bit).  For callers that need
+ * many instances' fields quickly (batched and served workloads). */
+int sdg_box_fields(int NeX, int NeY, int NeZ, int p, const double* x1D,
+                   int ic_kind, unsigned long long seed, int vel_kind,
+                   double vx, double vy, double vz, double* q, double* u,
+                   double* v, double* w);
+
 /* A constant velocity drawn from U[-1,1]^3 by a splitmix64 stream. */
 int sdg_random_velocity(unsigned long long seed, double* vel3);
 

@@ -780,19 +780,18 @@ int sdg_batch_destroy(sdg_batch* b) {
 // ===========================================================================
 // Serving loop
 // ===========================================================================
-// A worker thread owns the GPU side and advances the admitted requests in
-// chunks of RK steps.  Each chunk replays the CUDA graph of one RK step of
-// the current membership (all orders and sizes in one fork/join of batched
-// launches) n times, n = min(kChunkSteps, the fewest steps any member has
-// left), so no member overruns and the host meets the GPU once per chunk,
-// not once per step.  While a chunk runs, the worker
-//   * admits queued requests in arrival order while their device memory
-//     fits under the byte cap, uploading them on a copy stream of their own
-//     (the running chunk is not stalled by the uploads), and
-//   * copies out the results of the requests that the previous chunk
-//     finished, again on the copy stream, and returns their memory.
-// At the chunk boundary it reads the status word of the bounded waits once,
-// updates the membership (finished requests leave, admitted ones join),
+// Two threads own the GPU side.  The uploader admits queued requests in
+// arrival order while their device memory fits under the byte cap and
+// uploads each on a stream of its own, so neither the running chunk nor the
+// worker waits for host-to-device copies.  The worker advances the admitted
+// requests in chunks of RK steps.  Each chunk replays the CUDA graph of one
+// RK step of the current membership (all orders and sizes in one fork/join
+// of batched launches) n times, n = min(steps that fit in about kChunkMs of
+// device time, the fewest steps any member has left), so no member overruns
+// and the host meets the GPU once per chunk, not once per step.  At the
+// chunk boundary the worker reads the status word of the bounded waits once,
+// copies out the results of the members that chunk finished (on a third
+// stream) and returns their memory, lets the uploaded requests join,
 // re-captures the step graph if the membership changed, and launches the
 // next chunk.  Requests that arrive while others run join at the next chunk
 // boundary, so their work overlaps the others' on the device.
@@ -810,10 +809,14 @@ struct sdg_server {
   size_t cap = 0;
   size_t used = 0;
   std::mutex mu;
-  std::condition_variable cv;      // work arrived / stop
+  std::condition_variable cv;      // worker: uploaded requests, stop
+  std::condition_variable up_cv;   // uploader: a request queued, memory freed, stop
   std::condition_variable done_cv; // a request finished
   std::deque<Inst*> queue;
   std::vector<Inst*> active;       // members of the running chunk's graph
+  std::vector<Inst*> joining;      // uploaded, joining at the next chunk
+  int uploading = 0;               // admitted, upload in progress
+  bool chunk_running = false;
   std::map<int, std::unique_ptr<Inst>> all;
   // Operators of queued requests, by request (guarded by mu, like queue).
   std::map<const Inst*, PendingOps> pending_ops;
@@ -821,106 +824,104 @@ struct sdg_server {
   bool stop = false;
   int error = SDG_OK;
   std::string error_msg;
-  std::thread worker;
+  std::thread worker, uploader;
   double busy = 0;            // seconds of device time of the chunks
   long long dof_steps = 0;    // DOF x RK steps completed
   long long steps_run = 0;    // RK steps run (over all chunks)
   long long chunks = 0;
+  // The ensemble's operator and group tables: ops_for and group_for (the
+  // uploader) against the worker's use of the groups.
+  std::mutex ens_mu;
 
-  // Worker-only state (no lock needed).
-  cudaStream_t copy = nullptr;       // uploads and result downloads
+  // Worker-only state.
+  cudaStream_t up_stream = nullptr;  // uploads (uploader thread)
+  cudaStream_t out_stream = nullptr; // result downloads (worker)
   cudaGraphExec_t graph = nullptr;   // one RK step of `active`
   bool graph_stale = true;
   cudaEvent_t c0 = nullptr, c1 = nullptr;  // brackets of the running chunk
-  bool chunk_running = false;
   int chunk_steps = 0;
   double step_ms = 0;                // device time per step of the last chunk
-  std::vector<Inst*> joining;        // admitted, uploaded, not yet members
 
   ~sdg_server() {
     if (graph) cudaGraphExecDestroy(graph);
     if (c0) cudaEventDestroy(c0);
     if (c1) cudaEventDestroy(c1);
-    if (copy) cudaStreamDestroy(copy);
+    if (up_stream) cudaStreamDestroy(up_stream);
+    if (out_stream) cudaStreamDestroy(out_stream);
   }
 
   int init_worker_state() {
-    ENS_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+    ENS_CUDA(cudaStreamCreateWithFlags(&up_stream, cudaStreamNonBlocking));
+    ENS_CUDA(cudaStreamCreateWithFlags(&out_stream, cudaStreamNonBlocking));
     ENS_CUDA(cudaEventCreate(&c0));
     ENS_CUDA(cudaEventCreate(&c1));
     return SDG_OK;
   }
 
+  bool idle() const {
+    return queue.empty() && uploading == 0 && joining.empty() && active.empty() &&
+           !chunk_running;
+  }
+
+  void upload_loop();
+
   void loop() {
     cudaSetDevice(ens.dev);
     for (;;) {
-      std::vector<Inst*> admit;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv.wait(lk, [&] {
-          return stop || !queue.empty() || !active.empty() || !joining.empty() ||
-                 chunk_running;
+          return stop || !active.empty() || !joining.empty() || chunk_running;
         });
         if (stop) return;
-        while (!queue.empty() && used + queue.front()->bytes <= cap) {
-          Inst* I = queue.front();
-          queue.pop_front();
-          used += I->bytes;
-          admit.push_back(I);
-        }
       }
-      // Only this thread touches the ensemble (operators, groups, device
-      // memory); submitters only touch the queue under the lock.
-      admit_requests(admit);
+      // Only the worker changes the membership and launches; the uploader
+      // only adds operators and groups (under ens_mu) and uploads.
       finish_chunk();
       launch_chunk();
     }
   }
 
   void fail_all(int rc);
-  void admit_requests(std::vector<Inst*>& admit);
   void finish_chunk();
   void launch_chunk();
 };
 
-// Fails every request on the device after an error (the worker keeps
-// serving later submissions).
-void sdg_server::fail_all(int rc) {
-  std::lock_guard<std::mutex> lk(mu);
-  error = rc;
-  error_msg = last_error();
-  for (auto* list : {&active, &joining})
-    for (Inst* I : *list) {
-      ens.leave(I);
-      ens.release(I, ens.stream);
-      used -= I->bytes;
-      I->state = kFailed;
-    }
-  active.clear();
-  joining.clear();
-  graph_stale = true;
-  done_cv.notify_all();
-}
-
-// Uploads the admitted requests on the copy stream (the running chunk goes
-// on) and queues them to join at the next chunk boundary.
-void sdg_server::admit_requests(std::vector<Inst*>& admit) {
-  for (Inst* I : admit) {
-    int rc;
-    Ops* o = nullptr;
-    Group* g = nullptr;
+// Admits queued requests in arrival order while they fit under the cap and
+// uploads them; uploaded requests join at the worker's next chunk boundary.
+void sdg_server::upload_loop() {
+  cudaSetDevice(ens.dev);
+  for (;;) {
+    Inst* I = nullptr;
     PendingOps po;
     {
-      std::lock_guard<std::mutex> lk(mu);
+      std::unique_lock<std::mutex> lk(mu);
+      up_cv.wait(lk, [&] {
+        return stop || (!queue.empty() && used + queue.front()->bytes <= cap);
+      });
+      if (stop) return;
+      I = queue.front();
+      queue.pop_front();
+      used += I->bytes;
+      ++uploading;
+      I->t_admit = now_s();
       po = std::move(pending_ops[I]);
       pending_ops.erase(I);
     }
-    rc = ens.ops_for(I->p, po.D.data(), po.L.data(), &o);
-    if (!rc) rc = ens.group_for(I->nq, I->mixed, o, &g);
+    int rc;
+    {
+      std::lock_guard<std::mutex> lk(ens_mu);
+      Ops* o = nullptr;
+      Group* g = nullptr;
+      rc = ens.ops_for(I->p, po.D.data(), po.L.data(), &o);
+      if (!rc) rc = ens.group_for(I->nq, I->mixed, o, &g);
+    }
     if (!rc) rc = ens.upload(I, I->host[0].data(), I->host[1].data(), I->host[2].data(),
-                             I->host[3].data(), copy);
+                             I->host[3].data(), up_stream);
     std::lock_guard<std::mutex> lk(mu);
+    --uploading;
     if (rc) {
+      ens.release(I, up_stream);
       I->state = kFailed;
       used -= I->bytes;
       error = rc;
@@ -930,14 +931,36 @@ void sdg_server::admit_requests(std::vector<Inst*>& admit) {
     }
     for (auto& h : I->host) std::vector<double>().swap(h);
     I->state = kRunning;
-    I->t_admit = now_s();
     joining.push_back(I);
+    cv.notify_all();
   }
 }
 
+// Fails every request on the device after an error (the worker keeps
+// serving later submissions).
+void sdg_server::fail_all(int rc) {
+  std::lock_guard<std::mutex> el(ens_mu);
+  std::lock_guard<std::mutex> lk(mu);
+  error = rc;
+  error_msg = last_error();
+  for (auto* list : {&active, &joining})
+    for (Inst* I : *list) {
+      ens.leave(I);
+      ens.release(I, out_stream);
+      used -= I->bytes;
+      I->state = kFailed;
+    }
+  active.clear();
+  joining.clear();
+  chunk_running = false;
+  graph_stale = true;
+  up_cv.notify_all();
+  done_cv.notify_all();
+}
+
 // Waits for the running chunk, accounts it, retires the members it
-// finished (results copied out on the copy stream, memory returned) and
-// lets the admitted requests join.
+// finished (results copied out on the output stream, memory returned) and
+// lets the uploaded requests join.
 void sdg_server::finish_chunk() {
   if (chunk_running) {
     cudaError_t ce = cudaEventSynchronize(c1);
@@ -953,7 +976,6 @@ void sdg_server::finish_chunk() {
       busy += 1e-3 * ms;
       steps_run += chunk_steps;
       ++chunks;
-      if (rc) chunk_running = false;
     }
     if (rc) {
       fail_all(rc);
@@ -966,23 +988,26 @@ void sdg_server::finish_chunk() {
       I->steps_left -= chunk_steps;
       (I->steps_left > 0 ? keep : done).push_back(I);
     }
-    for (Inst* I : done) {
-      ens.leave(I);
-      graph_stale = true;
+    {
+      std::lock_guard<std::mutex> el(ens_mu);
+      for (Inst* I : done) {
+        ens.leave(I);
+        graph_stale = true;
+      }
     }
     {
       std::lock_guard<std::mutex> lk(mu);  // `active` is read by sdg_serve_wait
       active.swap(keep);
     }
-    // Results of the finished members, then their memory, on the copy
-    // stream; the next chunk (compute stream) no longer touches them.
+    // Results of the finished members, then their memory; the next chunk
+    // (compute stream) no longer touches them.
     for (Inst* I : done) {
       I->result.resize(static_cast<size_t>(I->np) * I->ne);
       cudaMemcpyAsync(I->result.data(), I->q0, I->result.size() * sizeof(double),
-                      cudaMemcpyDeviceToHost, copy);
-      ens.release(I, copy);
+                      cudaMemcpyDeviceToHost, out_stream);
+      ens.release(I, out_stream);
     }
-    if (!done.empty()) cudaStreamSynchronize(copy);
+    if (!done.empty()) cudaStreamSynchronize(out_stream);
     std::lock_guard<std::mutex> lk(mu);
     dof_steps += dof * chunk_steps;
     for (Inst* I : done) {
@@ -991,17 +1016,20 @@ void sdg_server::finish_chunk() {
       I->state = kDone;
     }
     chunk_running = false;
+    if (!done.empty()) up_cv.notify_all();
     done_cv.notify_all();
   }
-  std::lock_guard<std::mutex> lk(mu);
-  if (!joining.empty()) {
-    for (Inst* I : joining) {
-      Group* g = ens.groups.at(std::make_pair(I->nq, I->mixed)).get();
-      ens.join(I, g);
-      active.push_back(I);
-    }
-    joining.clear();
+  std::vector<Inst*> join;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    join.swap(joining);
+  }
+  if (!join.empty()) {
+    std::lock_guard<std::mutex> el(ens_mu);
+    for (Inst* I : join) ens.join(I, ens.groups.at(std::make_pair(I->nq, I->mixed)).get());
     graph_stale = true;
+    std::lock_guard<std::mutex> lk(mu);
+    active.insert(active.end(), join.begin(), join.end());
   }
 }
 
@@ -1018,6 +1046,7 @@ void sdg_server::launch_chunk() {
     return;
   }
   int rc = SDG_OK;
+  std::unique_lock<std::mutex> el(ens_mu);
   if (graph_stale) {
     if (graph) {
       cudaGraphExecDestroy(graph);
@@ -1044,11 +1073,13 @@ void sdg_server::launch_chunk() {
     }
     if (gr) cudaGraphDestroy(gr);
     if (rc) {
+      el.unlock();
       fail_all(rc);
       return;
     }
     graph_stale = false;
   }
+  el.unlock();
   long long n = kChunkSteps;
   if (step_ms > 0) n = std::max(1LL, std::min(n, static_cast<long long>(kChunkMs / step_ms)));
   for (Inst* I : active) n = std::min(n, I->steps_left);
@@ -1085,6 +1116,7 @@ int sdg_serve_create(sdg_server** out, double max_bytes) {
   if ((rc = s->init_worker_state())) return rc;
   sdg_server* raw = s.release();
   raw->worker = std::thread([raw] { raw->loop(); });
+  raw->uploader = std::thread([raw] { raw->upload_loop(); });
   *out = raw;
   return SDG_OK;
 }
@@ -1121,7 +1153,7 @@ int sdg_serve_submit(sdg_server* s, int NeX, int NeY, int NeZ, int p, const doub
   s->queue.push_back(I.get());
   *id = I->id;
   s->all[I->id] = std::move(I);
-  s->cv.notify_all();
+  s->up_cv.notify_all();
   return SDG_OK;
 }
 
@@ -1159,9 +1191,7 @@ int sdg_serve_wait(sdg_server* s, double timeout_s) {
   std::unique_lock<std::mutex> lk(s->mu);
   const auto deadline = std::chrono::steady_clock::now() +
                         std::chrono::duration<double>(timeout_s > 0 ? timeout_s : 1e9);
-  auto idle = [&] {
-    return s->queue.empty() && s->active.empty() && s->joining.empty() && !s->chunk_running;
-  };
+  auto idle = [&] { return s->idle(); };
   if (!s->done_cv.wait_until(lk, deadline, idle))
     return fail(SDG_ERR_STATE, "requests still pending after %.1f s", timeout_s);
   if (s->error) return fail(s->error, "%s", s->error_msg.c_str());
@@ -1185,10 +1215,13 @@ int sdg_serve_destroy(sdg_server* s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
     s->cv.notify_all();
+    s->up_cv.notify_all();
   }
   if (s->worker.joinable()) s->worker.join();
+  if (s->uploader.joinable()) s->uploader.join();
   cudaSetDevice(s->ens.dev);
   cudaStreamSynchronize(s->ens.stream);
+  cudaStreamSynchronize(s->up_stream);
   for (Inst* I : s->active) s->ens.release(I, s->ens.stream);
   for (Inst* I : s->joining) s->ens.release(I, s->ens.stream);
   cudaStreamSynchronize(s->ens.stream);

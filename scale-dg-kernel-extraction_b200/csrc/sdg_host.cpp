@@ -286,16 +286,20 @@ int sdg_random_velocity(unsigned long long seed, double* vel3) {
   return SDG_OK;
 }
 
-int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
-                    double vx, double vy, double vz, const double* pos_en,
-                    int Np, int Ne, double* q, double* u, double* v,
-                    double* w) {
+}  // extern "C"
+
+namespace {
+
+// The initial condition and velocity at every node x of [0, NE), the node
+// position from pos(x, &px, &py, &pz).  Nodes are independent, so they are
+// split over host threads (the values do not depend on the split).
+template <typename Pos>
+int fill_fields(int ic_kind, unsigned long long seed, int vel_kind, double vx, double vy,
+                double vz, long NE, Pos pos, double* q, double* u, double* v, double* w) {
   if (ic_kind < 0 || ic_kind > 1)
     return fail(SDG_ERR_ARG, "unknown initial-condition kind %d", ic_kind);
   if (vel_kind < 0 || vel_kind > 1)
     return fail(SDG_ERR_ARG, "unknown velocity kind %d", vel_kind);
-  if (!pos_en || !q || !u || !v || !w || Np < 1 || Ne < 1)
-    return fail(SDG_ERR_ARG, "sdg_init_fields: bad argument");
   const double pi = 4.0 * std::atan(1.0);  // mod_common.f90:25
   const double two_pi = 2.0 * pi;
   double kx[8], ky[8], kz[8], amp[8], ph[8];
@@ -307,33 +311,31 @@ int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
     amp[m] = 0.01 * r.gaussian(two_pi);
     ph[m] = two_pi * r.uniform();
   }
-  const long NE = static_cast<long>(Np) * Ne;
   const double two_s2 = 2.0 * 0.1 * 0.1;  // 2 sigma^2, sigma = 0.1
-  // Every node is independent: split the nodes over host threads (the
-  // values do not depend on the split).
   auto fill = [&](long x0, long x1) {
-  for (long x = x0; x < x1; ++x) {
-    const double px = pos_en[x], py = pos_en[x + NE], pz = pos_en[x + 2 * NE];
-    if (ic_kind == 0) {
-      q[x] = std::sin(two_pi * px) * std::sin(two_pi * py) * std::sin(two_pi * pz);
-    } else {
-      const double r2 = (px - 0.5) * (px - 0.5) + (py - 0.5) * (py - 0.5) +
-                        (pz - 0.5) * (pz - 0.5);
-      double s = std::exp(-r2 / two_s2);
-      for (int m = 0; m < 8; ++m)
-        s = s + amp[m] * std::cos(two_pi * (kx[m] * px + ky[m] * py + kz[m] * pz) + ph[m]);
-      q[x] = s;
+    for (long x = x0; x < x1; ++x) {
+      double px, py, pz;
+      pos(x, &px, &py, &pz);
+      if (ic_kind == 0) {
+        q[x] = std::sin(two_pi * px) * std::sin(two_pi * py) * std::sin(two_pi * pz);
+      } else {
+        const double r2 = (px - 0.5) * (px - 0.5) + (py - 0.5) * (py - 0.5) +
+                          (pz - 0.5) * (pz - 0.5);
+        double s = std::exp(-r2 / two_s2);
+        for (int m = 0; m < 8; ++m)
+          s = s + amp[m] * std::cos(two_pi * (kx[m] * px + ky[m] * py + kz[m] * pz) + ph[m]);
+        q[x] = s;
+      }
+      if (vel_kind == 0) {
+        u[x] = vx;
+        v[x] = vy;
+        w[x] = vz;
+      } else {
+        u[x] = std::sin(two_pi * py);
+        v[x] = std::sin(two_pi * pz);
+        w[x] = std::sin(two_pi * px);
+      }
     }
-    if (vel_kind == 0) {
-      u[x] = vx;
-      v[x] = vy;
-      w[x] = vz;
-    } else {
-      u[x] = std::sin(two_pi * py);
-      v[x] = std::sin(two_pi * pz);
-      w[x] = std::sin(two_pi * px);
-    }
-  }
   };
   const unsigned hw = std::thread::hardware_concurrency();
   const long nthr = std::max(1L, std::min({static_cast<long>(hw ? hw : 1), 32L, NE / 65536}));
@@ -347,5 +349,61 @@ int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
   }
   return SDG_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+int sdg_init_fields(int ic_kind, unsigned long long seed, int vel_kind,
+                    double vx, double vy, double vz, const double* pos_en,
+                    int Np, int Ne, double* q, double* u, double* v,
+                    double* w) {
+  if (!pos_en || !q || !u || !v || !w || Np < 1 || Ne < 1)
+    return fail(SDG_ERR_ARG, "sdg_init_fields: bad argument");
+  const long NE = static_cast<long>(Np) * Ne;
+  return fill_fields(ic_kind, seed, vel_kind, vx, vy, vz, NE,
+                     [&](long x, double* px, double* py, double* pz) {
+                       *px = pos_en[x];
+                       *py = pos_en[x + NE];
+                       *pz = pos_en[x + 2 * NE];
+                     },
+                     q, u, v, w);
+}
+
+int sdg_box_fields(int NeX, int NeY, int NeZ, int p, const double* x1D, int ic_kind,
+                   unsigned long long seed, int vel_kind, double vx, double vy, double vz,
+                   double* q, double* u, double* v, double* w) {
+  int sz[6];
+  int rc = sdg_mesh_sizes(NeX, NeY, NeZ, p, sz);
+  if (rc) return rc;
+  if (!x1D || !q || !u || !v || !w) return fail(SDG_ERR_ARG, "sdg_box_fields: null array");
+  const int Ne = sz[0], Np = sz[4];
+  const int Nq = p + 1, Nfp = Nq * Nq;
+  const double h[3] = {1.0 / static_cast<double>(NeX), 1.0 / static_cast<double>(NeY),
+                       1.0 / static_cast<double>(NeZ)};
+  const long NE = static_cast<long>(Np) * Ne;
+  // The node positions of sdg_mesh_setup on the unit box, computed where
+  // they are used: element centre (i - 1/2) h (1-based i) plus h/2 x1D.
+  return fill_fields(ic_kind, seed, vel_kind, vx, vy, vz, NE,
+                     [&](long x, double* px, double* py, double* pz) {
+                       const long e = x / Np;
+                       const int n = static_cast<int>(x - e * Np);
+                       const long ej = e / NeX;
+                       const int el[3] = {static_cast<int>(e - ej * NeX) + 1,
+                                          static_cast<int>(ej % NeY) + 1,
+                                          static_cast<int>(ej / NeY) + 1};
+                       const int ix[3] = {n % Nq, (n / Nq) % Nq, n / Nfp};
+                       double r3[3];
+                       for (int d = 0; d < 3; ++d)
+                         r3[d] = (static_cast<double>(el[d]) - 0.5) * h[d] +
+                                 0.5 * h[d] * x1D[ix[d]];
+                       *px = r3[0];
+                       *py = r3[1];
+                       *pz = r3[2];
+                     },
+                     q, u, v, w);
+}
+
+
 
 }  // extern "C"

@@ -109,8 +109,10 @@ int launch_tend(const LaunchSpec& s);
 
 // Kernel variants: the one-tile-per-block kernel (tend_kernel) and the
 // persistent bulk-copy pipelined kernel (tend_pipe_kernel); identical
-// arithmetic.  Auto picks the pipelined one when its shared-memory plan fits
-// one block (kPipeMaxSmem) and every array is 16-byte aligned.
+// arithmetic.  Auto picks the split-column kernel at the orders where it
+// measured faster (kSplitAuto), else the pipelined one when its
+// shared-memory plan fits one block (kPipeMaxSmem) and every array is
+// 16-byte aligned, else the one-tile-per-block kernel.
 // kVariantBlockOcc is the one-tile-per-block kernel built for eight resident
 // blocks per SM (p = 3..7; other orders use kVariantBlock).
 // kVariantSplit is the persistent ring kernel with each z-column split over

@@ -99,8 +99,11 @@ int run(const LaunchSpec& s) {
                            (EXACT || s.lift_z != nullptr) &&
                            (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
                                       aligned(s.w) && aligned(s.escale) &&
-                                      aligned(s.fscale)));
-    if (s.variant == kVariantSplit) {
+                                      aligned(s.fscale) && aligned(s.pbase)));
+    const bool want_split =
+        s.variant == kVariantSplit ||
+        (s.variant == kVariantAuto && !batch && kSplitAuto<NQ, TC, EXACT>);
+    if (want_split) {
       if (!can_split) {
         if (batch) return static_cast<int>(cudaErrorNotSupported);
       } else {

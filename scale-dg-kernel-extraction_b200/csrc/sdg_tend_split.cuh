@@ -38,9 +38,14 @@ struct SplitGeo {
   static constexpr int KZ = (NQ + H - 1) / H;  // column nodes per thread
 };
 
-// Shared-memory plan: the ring of one-element slots, the minus-side face
-// values (FaceArea), the face fluxes ((f1, f3) and (f2, f4) pairs per face
-// node, f5 and f6 per column), the factored lift's x/y factors, barriers.
+// Shared-memory plan: the ring of one-element slots (q, u, v, w and the
+// element's escale, fscale and face-neighbour rows), the x- and y-line
+// buffers, the minus-side face values (FaceArea), the face fluxes ((f1, f3)
+// and (f2, f4) pairs per face node, f5 and f6 per column), the factored
+// lift's x/y factors, barriers.  The line buffers have space of their own
+// (SEP) where the plan fits, so phase 1 writes them directly; otherwise they
+// reuse the slot's u and v regions once every thread holds its column,
+// which costs a barrier.
 template <int NQ, int H, typename TQ, typename TV, typename TC, bool STAGE>
 struct SplitPlan {
   static constexpr int NQ2 = NQ * NQ;
@@ -48,23 +53,42 @@ struct SplitPlan {
   static constexpr int NSTAGE = 2;
   static constexpr size_t r16(size_t x) { return (x + 15) & ~size_t(15); }
   static constexpr size_t mx(size_t a, size_t b) { return a > b ? a : b; }
+  static constexpr size_t LINE =
+      r16(sizeof(TC) * LineIdx<NQ, static_cast<int>(sizeof(TC))>::SIZE);
   static constexpr size_t QB = r16(sizeof(TQ) * NP + 32);
-  static constexpr size_t VB =
-      mx(r16(sizeof(TV) * NP + 32),
-         r16(sizeof(TC) * LineIdx<NQ, static_cast<int>(sizeof(TC))>::SIZE));
+  static constexpr size_t VB0 = r16(sizeof(TV) * NP + 32);
   static constexpr size_t EB = r16(sizeof(TC) * 3 + 32);
   static constexpr size_t FB = r16(sizeof(TC) * 6 + 32);
+  static constexpr size_t PB = r16(sizeof(int) * 6 + 32);
+  static constexpr size_t FACE = r16(sizeof(TC) * FaceArea<NQ, sizeof(TC) == 8>::ELEM);
+  static constexpr size_t FLUX = r16(sizeof(TC) * 6 * NQ2);
+  static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
+  static constexpr size_t BARS = 16 * NSTAGE;
+  static constexpr size_t REST = FACE + FLUX + LIFTB + BARS;
+  static constexpr size_t SEP_BYTES =
+      NSTAGE * (QB + 3 * VB0 + EB + FB + PB) + 2 * LINE + REST;
+  static constexpr size_t ALIAS_BYTES = NSTAGE * (QB + 3 * mx(VB0, LINE) + EB + FB + PB) + REST;
+  static constexpr int blocks(size_t bytes) {
+    return static_cast<int>(kSmemPerSM / (bytes + kSmemPerBlockReserved));
+  }
+  // Resident blocks the registers allow (at least 128 registers per FP64
+  // thread, 80 per FP32 thread; see split_min_blocks).
+  static constexpr int REG_BLOCKS =
+      65536 / (((H * NQ2 + 31) / 32 * 32) * (sizeof(TC) == 8 ? 128 : 80));
+  static constexpr int cap(int b) { return b < REG_BLOCKS ? b : REG_BLOCKS; }
+  // Separate line buffers where they fit and cost no resident block.
+  static constexpr bool SEP =
+      SEP_BYTES <= kPipeMaxSmem && cap(blocks(SEP_BYTES)) >= cap(blocks(ALIAS_BYTES));
+  static constexpr size_t VB = SEP ? VB0 : mx(VB0, LINE);
   static constexpr size_t OFF_U = QB;
   static constexpr size_t OFF_V = QB + VB;
   static constexpr size_t OFF_W = QB + 2 * VB;
   static constexpr size_t OFF_E = QB + 3 * VB;
   static constexpr size_t OFF_F = OFF_E + EB;
-  static constexpr size_t SLOT = OFF_F + FB;
-  static constexpr size_t FACE = r16(sizeof(TC) * FaceArea<NQ, sizeof(TC) == 8>::ELEM);
-  static constexpr size_t FLUX = r16(sizeof(TC) * 6 * NQ2);
-  static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
-  static constexpr size_t BARS = 16 * NSTAGE;
-  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + FLUX + LIFTB + BARS;
+  static constexpr size_t OFF_P = OFF_F + FB;
+  static constexpr size_t SLOT = OFF_P + PB;
+  static constexpr size_t LINES = SEP ? 2 * LINE : 0;
+  static constexpr size_t BYTES = NSTAGE * SLOT + LINES + REST;
   static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
       kSmemPerSM / (BYTES + kSmemPerBlockReserved) > 4
           ? 4
@@ -76,6 +100,15 @@ struct SplitPlan {
 // Columns split in two from Nq = 9 on.
 template <int NQ>
 constexpr int kSplitH = 2;
+
+// Where the automatic variant takes the split-column kernel: the orders at
+// which it measured faster than tend_pipe_kernel (RK stage 2, ~16.8 M DOF,
+// ms split / pipelined): fast FP64 p = 8 0.266 / 0.271, p = 9 0.241 / 0.272,
+// p = 11 0.295 / 0.331, p = 12 0.310 / 0.344, p = 13 0.275 / 0.342; mixed
+// p = 11 0.144 / 0.151.  Slower at FP64 p = 10 and the other mixed orders.
+template <int NQ, typename TC, bool EXACT>
+constexpr bool kSplitAuto =
+    !EXACT && (sizeof(TC) == 8 ? (NQ == 9 || NQ == 10 || (NQ >= 12 && NQ <= 14)) : NQ == 12);
 
 // Blocks per SM the kernel is built for: what the shared memory allows,
 // capped so that a thread keeps at least 128 (FP64) or 80 (FP32) registers.
@@ -109,11 +142,12 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* slots = smem_raw;
-  TC* fa = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT);
-  TC* flux = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::FACE);
-  TC* sL = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::FACE + P::FLUX);
-  uint64_t* bars =
-      reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::FACE + P::FLUX + P::LIFTB);
+  unsigned char* rest = smem_raw + NS * P::SLOT + P::LINES;
+  TC* fa = reinterpret_cast<TC*>(rest);
+  TC* flux = reinterpret_cast<TC*>(rest + P::FACE);
+  TC* sL = reinterpret_cast<TC*>(rest + P::FACE + P::FLUX);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(rest + P::FACE + P::FLUX + P::LIFTB);
+  constexpr bool SEP = P::SEP;
 
   const int h = threadIdx.x / NQ2;      // part of the column
   const int c = threadIdx.x - h * NQ2;  // column a + NQ*b
@@ -146,20 +180,21 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     if (tile + 1 == A.inject_skip) return;
     const Ctx cx = tile_ctx<1, BATCH>(A, tile, ntiles);
     unsigned char* base = slots + slot * P::SLOT;
-    const void* src[6] = {cx.q, cx.u, cx.v, cx.w, cx.escale, cx.fscale};
-    const size_t per[6] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
-                           sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6};
-    const size_t off[6] = {0, P::OFF_U, P::OFF_V, P::OFF_W, P::OFF_E, P::OFF_F};
-    size_t lo[6];
-    uint32_t by[6], sh[6], total = 0;
+    const void* src[7] = {cx.q, cx.u, cx.v, cx.w, cx.escale, cx.fscale, cx.pbase};
+    const size_t per[7] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
+                           sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6,
+                           sizeof(int) * 6};
+    const size_t off[7] = {0, P::OFF_U, P::OFF_V, P::OFF_W, P::OFF_E, P::OFF_F, P::OFF_P};
+    size_t lo[7];
+    uint32_t by[7], sh[7], total = 0;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < 7; ++k) {
       tile_range(cx.e0, cx.n, per[k], &lo[k], &by[k], &sh[k]);
       total += by[k];
     }
     mbar_arrive_expect_tx(&bars[slot], total);
 #pragma unroll
-    for (int k = 0; k < 6; ++k)
+    for (int k = 0; k < 7; ++k)
       bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
                &bars[slot]);
     if (STAGE && A.rk_a != 0.0) {
@@ -196,15 +231,6 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     const int e = C.e0;
     const long base = static_cast<long>(e) * NP;
 
-    // The faces this thread evaluates: their neighbour rows, needed after
-    // phase 1.
-    int pbc[6];
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      const bool mine = (f == 0 || f == 2 || f == 4) ? own_y : own_x;
-      pbc[f] = mine ? ldro(C.pbase + 6 * static_cast<long>(e) + f) : 0;
-    }
-
     // ---- Wait for the tile's slot (bounded, block-uniform) ---------------
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity, spins));
     if (!ok) {
@@ -232,31 +258,53 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     const TV* sw = reinterpret_cast<const TV*>(sb + P::OFF_W + shv);
     const TC* ses = reinterpret_cast<const TC*>(sb + P::OFF_E + tile_shift(C.e0, sizeof(TC) * 3));
     const TC* sfs = reinterpret_cast<const TC*>(sb + P::OFF_F + tile_shift(C.e0, sizeof(TC) * 6));
+    const int* spb = reinterpret_cast<const int*>(sb + P::OFF_P + tile_shift(C.e0, 24));
     static_assert(sizeof(TV) == sizeof(TC), "w and q*w share their slots");
     TC* sz = reinterpret_cast<TC*>(sb + P::OFF_W + shv);
-    TC* sX = reinterpret_cast<TC*>(sb + P::OFF_U);
-    TC* sY = reinterpret_cast<TC*>(sb + P::OFF_V);
+    TC* sX = SEP ? reinterpret_cast<TC*>(smem_raw + NS * P::SLOT)
+                 : reinterpret_cast<TC*>(sb + P::OFF_U);
+    TC* sY = SEP ? reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::LINE)
+                 : reinterpret_cast<TC*>(sb + P::OFF_V);
 
-    // ---- Plus-side face values, from global memory (L2) -------------------
-    // Slots 0, 1: the two x or y faces of this thread; 2: its z face.
+    // ---- Plus-side face values (L2) and q0, issued first ------------------
+    // The face-neighbour row came with the tile.  Slots 0, 1: the two x or y
+    // faces of this thread; 2: its z face.
     TC qP[3], unP[3];
-    auto gather = [&]() {
+    {
 #pragma unroll
       for (int f = 0; f < 6; ++f) {
         const bool mine = (f == 0 || f == 2 || f == 4) ? own_y : own_x;
         if (!mine) continue;
+        const int pb = spb[f];
         // slot of face f among this thread's faces
         const int sl = (f >= 4) ? 2 : ((f == 0 || f == 1) ? 0 : 1);
-        const long idx = (pbc[f] >= 0) ? static_cast<long>(pbc[f]) + opp_offset<NQ>(f, a, b)
-                                       : static_cast<long>(-1 - pbc[f]) + c;
+        const long idx = (pb >= 0) ? static_cast<long>(pb) + opp_offset<NQ>(f, a, b)
+                                   : static_cast<long>(-1 - pb) + c;
         qP[sl] = static_cast<TC>(ldro(C.q + idx));
         unP[sl] = static_cast<TC>((f == 1 || f == 3) ? ldro(C.u + idx)
                                                      : ((f >= 4) ? ldro(C.w + idx)
                                                                  : ldro(C.v + idx)));
       }
+    }
+    // q0 (RK stages 2-3, in L2 since the tile's copies were issued): loaded
+    // here where the separate line buffers leave registers to spare, after
+    // the lines otherwise (measured: FP64 p = 10, aliased plan, 0.33 against
+    // 0.25 ms with the early loads).
+    double q0r[STAGE ? KZ : 1];
+    const bool use_q0 = STAGE && A.rk_a != 0.0;
+    auto load_q0 = [&]() {
+      if constexpr (STAGE) {
+        if (use_q0) {
+#pragma unroll
+          for (int kk = 0; kk < KZ; ++kk) {
+            const int k = k0 + kk;
+            if (KZ * H != NQ && k >= NQ) break;
+            q0r[kk] = ld_stream(C.q0 + base + c + NQ2 * k);
+          }
+        }
+      }
     };
-    constexpr bool EARLY = sizeof(TC) == 8;
-    if constexpr (EARLY) gather();
+    if constexpr (SEP) load_q0();
 
     // ---- Phase 1: this thread's nodes of column c -------------------------
     TC fx[KZ], fy[KZ];
@@ -287,6 +335,10 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         fx[kk] = AR::mul(qv, uv);
         fy[kk] = AR::mul(qv, vv);
         sz[n] = AR::mul(qv, wv);
+        if constexpr (SEP) {
+          sX[LI::colx(a, b, k)] = fx[kk];
+          sY[LI::coly(a, b, k)] = fy[kk];
+        }
         if constexpr (XSPLIT) {
           if (onx) {
             xq[xo + NQ * k] = qv;
@@ -298,19 +350,22 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         if (ony) fmy[NQ * k] = V2{qv, vv};
       }
     }
-    __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
-#pragma unroll
-    for (int kk = 0; kk < KZ; ++kk) {
-      const int k = k0 + kk;
-      if (KZ * H != NQ && k >= NQ) break;
-      sX[LI::colx(a, b, k)] = fx[kk];
-      sY[LI::coly(a, b, k)] = fy[kk];
-    }
+    // The slot's writes (q*w; line buffers in u, v without SEP) come before
+    // the refill that overwrites it.
+    fence_proxy_async_smem();
     __syncthreads();
-    if constexpr (!EARLY) gather();
+    if constexpr (!SEP) {
+      // The slot's u, v are dead: reuse them as line buffers.
+#pragma unroll
+      for (int kk = 0; kk < KZ; ++kk) {
+        const int k = k0 + kk;
+        if (KZ * H != NQ && k >= NQ) break;
+        sX[LI::colx(a, b, k)] = fx[kk];
+        sY[LI::coly(a, b, k)] = fy[kk];
+      }
+      __syncthreads();
+    }
 
-    double q0r[STAGE ? KZ : 1];
-    const bool use_q0 = STAGE && A.rk_a != 0.0;
     // ---- Lines: x-line c (h = 0) and y-line c (h = 1), in place ----------
     {
       const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
@@ -333,17 +388,11 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
               [&](int l) { return line[l]; }, [&](int l) { return D.d[j * NQ + l]; });
       }
     }
-    // The line buffers live in the slot that the next refill overwrites.
-    fence_proxy_async_smem();
-    if constexpr (STAGE) {
-      if (use_q0) {
-#pragma unroll
-        for (int kk = 0; kk < KZ; ++kk) {
-          const int k = k0 + kk;
-          if (KZ * H != NQ && k >= NQ) break;
-          q0r[kk] = ld_stream(C.q0 + base + c + NQ2 * k);
-        }
-      }
+    // Without SEP the line buffers live in the slot that the next refill
+    // overwrites.
+    if constexpr (!SEP) {
+      fence_proxy_async_smem();
+      load_q0();
     }
     // ---- Face fluxes ------------------------------------------------------
     if (own_y) {

@@ -61,6 +61,7 @@ SIGNATURES = {
     "sdg_update_halo_host": (_I, [_P, _I, _I, _I, _P]),
     "sdg_init_fields": (_I, [_I, _U64, _I, _D, _D, _D, _P, _I, _I, _P, _P, _P, _P]),
     "sdg_random_velocity": (_I, [_U64, _P]),
+    "sdg_box_fields": (_I, [_I, _I, _I, _I, _P, _I, _U64, _I, _D, _D, _D, _P, _P, _P, _P]),
     "sdg_init": (_I, [ctypes.POINTER(_P), _I, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P,
                       _P, _P, _P, _I]),
     "sdg_finalize": (_I, [_P]),
@@ -209,15 +210,13 @@ def mesh_setup(NeX, NeY, NeZ, p, x1D, dom=(1.0, 1.0, 1.0)):
 
 def box_fields(NeX, NeY, NeZ, p, x1D, ic_kind=1, seed=0, vel_kind=0, vel=(1.0, 1.0, 1.0)):
     """Initial q, u, v, w (Np, Ne) of the periodic unit box without building
-    the mesh tables (only the node positions)."""
+    the mesh tables (sdg_box_fields: the same values as init_fields on
+    mesh_setup's positions)."""
     s = mesh_sizes(NeX, NeY, NeZ, p)
     Np, Ne = s["Np"], s["Ne"]
-    pos = np.zeros((Np, Ne, 3), order="F")
-    _check(lib().sdg_mesh_setup(NeX, NeY, NeZ, p, 1.0, 1.0, 1.0, _p(_f64(x1D)), None, None,
-                                None, None, None, None, _p(pos)))
-    q, u, v, w = (np.zeros((Np, Ne), order="F") for _ in range(4))
-    _check(lib().sdg_init_fields(ic_kind, seed, vel_kind, vel[0], vel[1], vel[2], _p(pos),
-                                 Np, Ne, _p(q), _p(u), _p(v), _p(w)))
+    q, u, v, w = (np.empty((Np, Ne), order="F") for _ in range(4))
+    _check(lib().sdg_box_fields(NeX, NeY, NeZ, p, _p(_f64(x1D)), ic_kind, seed, vel_kind,
+                                vel[0], vel[1], vel[2], _p(q), _p(u), _p(v), _p(w)))
     return q, u, v, w
 
 

@@ -92,3 +92,17 @@ def test_update_halo_host():
     sdg.update_halo(f, m)
     orc.update_halo(g, orc.mesh_setup(2, 3, 2, p, x1D))
     assert np.array_equal(f, g)
+
+
+@pytest.mark.parametrize("dims,p,vel_kind", [((3, 4, 5), 3, 0), ((2, 3, 2), 9, 1),
+                                             ((5, 2, 3), 1, 1), ((1, 1, 1), 15, 0)])
+def test_box_fields_equal_init_fields_on_mesh_positions(dims, p, vel_kind):
+    """sdg_box_fields forms the node positions where it uses them; the fields
+    equal sdg_init_fields on mesh_setup's pos_en bit for bit."""
+    ops = sdg.read_operators(p)
+    f1 = sdg.box_fields(*dims, p, ops.x1D, ic_kind=1, seed=7, vel_kind=vel_kind,
+                        vel=(0.3, -0.2, 0.9))
+    m = sdg.mesh_setup(*dims, p, ops.x1D)
+    f2 = sdg.init_fields(m, ic_kind=1, seed=7, vel_kind=vel_kind, vel=(0.3, -0.2, 0.9))
+    for a, b in zip(f1, f2):
+        assert np.array_equal(a, b[:, : m.Ne])
