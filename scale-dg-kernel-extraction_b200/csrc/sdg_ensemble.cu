@@ -816,6 +816,7 @@ struct sdg_server {
   std::vector<Inst*> active;       // members of the running chunk's graph
   std::vector<Inst*> joining;      // uploaded, joining at the next chunk
   int uploading = 0;               // admitted, upload in progress
+  int retiring = 0;                // finished, results being copied out
   bool chunk_running = false;
   std::map<int, std::unique_ptr<Inst>> all;
   // Operators of queued requests, by request (guarded by mu, like queue).
@@ -860,7 +861,7 @@ struct sdg_server {
 
   bool idle() const {
     return queue.empty() && uploading == 0 && joining.empty() && active.empty() &&
-           !chunk_running;
+           !chunk_running && retiring == 0;
   }
 
   void upload_loop();
@@ -876,15 +877,19 @@ struct sdg_server {
         if (stop) return;
       }
       // Only the worker changes the membership and launches; the uploader
-      // only adds operators and groups (under ens_mu) and uploads.
-      finish_chunk();
+      // only adds operators and groups (under ens_mu) and uploads.  The
+      // results of the finished members are copied out while the next
+      // chunk runs.
+      std::vector<Inst*> done = finish_chunk();
       launch_chunk();
+      retire(done);
     }
   }
 
   void fail_all(int rc);
-  void finish_chunk();
+  std::vector<Inst*> finish_chunk();
   void launch_chunk();
+  void retire(std::vector<Inst*>& done);
 };
 
 // Admits queued requests in arrival order while they fit under the cap and
@@ -958,10 +963,11 @@ void sdg_server::fail_all(int rc) {
   done_cv.notify_all();
 }
 
-// Waits for the running chunk, accounts it, retires the members it
-// finished (results copied out on the output stream, memory returned) and
-// lets the uploaded requests join.
-void sdg_server::finish_chunk() {
+// Waits for the running chunk, accounts it, takes the members it finished
+// out of their groups (returned, for retire) and lets the uploaded requests
+// join.
+std::vector<Inst*> sdg_server::finish_chunk() {
+  std::vector<Inst*> done;
   if (chunk_running) {
     cudaError_t ce = cudaEventSynchronize(c1);
     float ms = 0;
@@ -979,9 +985,9 @@ void sdg_server::finish_chunk() {
     }
     if (rc) {
       fail_all(rc);
-      return;
+      return done;
     }
-    std::vector<Inst*> keep, done;
+    std::vector<Inst*> keep;
     long long dof = 0;
     for (Inst* I : active) {
       dof += static_cast<long long>(I->np) * I->ne;
@@ -995,29 +1001,11 @@ void sdg_server::finish_chunk() {
         graph_stale = true;
       }
     }
-    {
-      std::lock_guard<std::mutex> lk(mu);  // `active` is read by sdg_serve_wait
-      active.swap(keep);
-    }
-    // Results of the finished members, then their memory; the next chunk
-    // (compute stream) no longer touches them.
-    for (Inst* I : done) {
-      I->result.resize(static_cast<size_t>(I->np) * I->ne);
-      cudaMemcpyAsync(I->result.data(), I->q0, I->result.size() * sizeof(double),
-                      cudaMemcpyDeviceToHost, out_stream);
-      ens.release(I, out_stream);
-    }
-    if (!done.empty()) cudaStreamSynchronize(out_stream);
-    std::lock_guard<std::mutex> lk(mu);
+    std::lock_guard<std::mutex> lk(mu);  // `active` is read by sdg_serve_wait
+    active.swap(keep);
+    retiring += static_cast<int>(done.size());
     dof_steps += dof * chunk_steps;
-    for (Inst* I : done) {
-      used -= I->bytes;
-      I->t_done = now_s();
-      I->state = kDone;
-    }
     chunk_running = false;
-    if (!done.empty()) up_cv.notify_all();
-    done_cv.notify_all();
   }
   std::vector<Inst*> join;
   {
@@ -1031,6 +1019,29 @@ void sdg_server::finish_chunk() {
     std::lock_guard<std::mutex> lk(mu);
     active.insert(active.end(), join.begin(), join.end());
   }
+  return done;
+}
+
+// Copies the finished members' results to the host on the output stream and
+// returns their memory; the running chunk no longer touches them.
+void sdg_server::retire(std::vector<Inst*>& done) {
+  if (done.empty()) return;
+  for (Inst* I : done) {
+    I->result.resize(static_cast<size_t>(I->np) * I->ne);
+    cudaMemcpyAsync(I->result.data(), I->q0, I->result.size() * sizeof(double),
+                    cudaMemcpyDeviceToHost, out_stream);
+    ens.release(I, out_stream);
+  }
+  cudaStreamSynchronize(out_stream);
+  std::lock_guard<std::mutex> lk(mu);
+  for (Inst* I : done) {
+    used -= I->bytes;
+    I->t_done = now_s();
+    I->state = kDone;
+  }
+  retiring -= static_cast<int>(done.size());
+  up_cv.notify_all();
+  done_cv.notify_all();
 }
 
 // Re-captures the step graph if the membership changed and launches the

@@ -581,6 +581,7 @@ int sdg_init(sdg_handle** out, int Nq, int Np, int NfpTot, int Ne, int NeA,
     else if (kv && std::strcmp(kv, "pipe") == 0) h->variant = kVariantPipe;
     else if (kv && std::strcmp(kv, "blockocc") == 0) h->variant = kVariantBlockOcc;
     else if (kv && std::strcmp(kv, "split") == 0) h->variant = kVariantSplit;
+    else if (kv && std::strcmp(kv, "tensor") == 0) h->variant = kVariantTensor;
   }
 
   auto bail = [&](int code) { free_handle(h); return code; };
@@ -897,9 +898,10 @@ long long sdg_launch_count(sdg_handle* h) { return h ? h->launches : -1; }
 
 int sdg_set_kernel_variant(sdg_handle* h, int variant) {
   if (!h) return fail(SDG_ERR_ARG, "null handle");
-  if (variant < kVariantAuto || variant > kVariantSplit)
+  if (variant < kVariantAuto || variant > kVariantTensor)
     return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block), 2 (pipelined), "
-                "3 (block, 8 blocks per SM) or 4 (pipelined, split columns)");
+                "3 (block, 8 blocks per SM), 4 (pipelined, split columns) or 5 "
+                "(pipelined, tensor-core lines of the mixed form at p = 7)");
   if (variant != h->variant && h->graph) {
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;

@@ -117,13 +117,17 @@ int launch_tend(const LaunchSpec& s);
 // blocks per SM (p = 3..7; other orders use kVariantBlock).
 // kVariantSplit is the persistent ring kernel with each z-column split over
 // two threads (tend_split_kernel), for the orders with one element per tile
-// (Nq >= 9).
+// (Nq >= 9).  kVariantTensor is the pipelined kernel of the mixed form at
+// Nq = 8 with its x/y lines on the tensor cores (TF32, three hi/lo passes);
+// its rounding differs from the other variants', so it is never chosen
+// automatically (other orders and forms run their automatic variant).
 enum KernelVariant {
   kVariantAuto = 0,
   kVariantBlock = 1,
   kVariantPipe = 2,
   kVariantBlockOcc = 3,
-  kVariantSplit = 4
+  kVariantSplit = 4,
+  kVariantTensor = 5
 };
 
 // Returns 0 when launched, -1 when this unit does not hold spec.nq,

@@ -117,10 +117,19 @@ int run(const LaunchSpec& s) {
       }
     }
   }
+  // Tensor-core lines (mixed form, Nq = 8, single instance).
+  if constexpr (NQ == 8 && sizeof(TC) == 4 && !EXACT && STAGE) {
+    using TP = PipePlan<NQ, TQ, TV, TC, STAGE, true>;
+    if (s.variant == kVariantTensor && !batch && can_pipe && TP::BYTES <= device_smem_optin()) {
+      const int ntiles = (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
+      return launch_pipe<tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false, true>>(
+          TP::BYTES, ntiles, s, a, d);
+    }
+  }
   if (batch && !can_pipe) return static_cast<int>(cudaErrorNotSupported);
   const bool pipe =
       batch || ((s.variant == kVariantPipe || s.variant == kVariantAuto ||
-                 s.variant == kVariantSplit) && can_pipe);
+                 s.variant == kVariantSplit || s.variant == kVariantTensor) && can_pipe);
   if (pipe) {
     const int ntiles =
         batch ? s.batch_ntiles : (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;

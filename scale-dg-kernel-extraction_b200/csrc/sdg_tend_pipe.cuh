@@ -41,6 +41,7 @@
 // __syncthreads_and so that no thread can skip a barrier another reaches.
 #pragma once
 
+#include "sdg_tcgen05.cuh"
 #include "sdg_tend.cuh"
 
 namespace sdg {
@@ -336,8 +337,10 @@ struct PipeGeo {
   static constexpr int THREADS = EPB * NQ2;
 };
 
-// Shared-memory plan of the pipelined kernel.
-template <int NQ, typename TQ, typename TV, typename TC, bool STAGE>
+// Shared-memory plan of the pipelined kernel.  TCG adds the operands of the
+// tensor-core line contractions (sdg_tcgen05.cuh): x and y, hi and lo, the
+// hi and lo halves of D, the TMEM address and the MMA completion barrier.
+template <int NQ, typename TQ, typename TV, typename TC, bool STAGE, bool TCG = false>
 struct PipePlan {
   using G = PipeGeo<NQ>;
   static constexpr int EPB = G::EPB;
@@ -366,7 +369,8 @@ struct PipePlan {
   // Per-face lift factors l_f(n) of the fast kernels, (4, Nq).
   static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
   static constexpr size_t BARS = 16 * NSTAGE;
-  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + LIFTB + BARS;
+  static constexpr size_t TCGB = TCG ? 4 * tc::kOperandBytes + 2 * tc::kBBytes + 32 : 0;
+  static constexpr size_t BYTES = NSTAGE * SLOT + FACE + LIFTB + BARS + TCGB;
   // Blocks per SM that the shared memory allows (the register budget per
   // thread follows from it), at most 4.
   static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
@@ -473,9 +477,10 @@ __device__ __forceinline__ uint32_t tile_shift(int e0, size_t per_elem) {
 // at Nq = 9) and for all columns of 12 or more nodes; and at most 3 for the
 // fast FP64 kernels at Nq = 7 (at the four-block budget of 128 registers they
 // spill 36 bytes; three blocks measured 10 % faster: 62.7 -> 69.1 G).
-template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE>
+template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE,
+          bool TCG = false>
 constexpr int pipe_min_blocks() {
-  constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE>::MIN_BLOCKS;
+  constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE, TCG>::MIN_BLOCKS;
   if constexpr (sizeof(TC) == 8 && !EXACT && NQ == 7) return m > 3 ? 3 : m;
   return ((EXACT || (sizeof(TC) == 8 && NQ >= 9) || NQ >= 12) && m > 2) ? 2 : m;
 }
@@ -483,14 +488,23 @@ constexpr int pipe_min_blocks() {
 // The thread bound is the block size rounded up to whole warps (the
 // compiler front end of CUDA 12.9 fails on this kernel with a bound of,
 // e.g., 81 threads at Nq = 9).
+//
+// TCG (mixed form at Nq = 8 only, kernel variant kVariantTensor): the x and
+// y line contractions on the tensor cores, TF32 in three hi/lo passes with
+// the results in tensor memory (sdg_tcgen05.cuh); phase 1 writes the split
+// operands, one thread issues the MMAs after the first barrier, and each
+// line owner reads its eight results back into the line buffers.  Its
+// rounding differs from the FP32 FMA lines of the other variants.
 template <int NQ, typename TQ, typename TV, typename TO, typename TC, bool EXACT,
-          int ORDER, bool STAGE, bool BATCH>
+          int ORDER, bool STAGE, bool BATCH, bool TCG = false>
 __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
-                                  (pipe_min_blocks<NQ, TQ, TV, TC, EXACT, STAGE>()))
+                                  (pipe_min_blocks<NQ, TQ, TV, TC, EXACT, STAGE, TCG>()))
     tend_pipe_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
                      const __grid_constant__ DMat<NQ, TC> D) {
   using G = PipeGeo<NQ>;
-  using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
+  using P = PipePlan<NQ, TQ, TV, TC, STAGE, TCG>;
+  static_assert(!TCG || (NQ == 8 && sizeof(TC) == 4 && !EXACT && G::THREADS == 128),
+                "tensor-core lines: fast FP32 at Nq = 8, 128 threads");
   using AR = Ar<TC, EXACT>;
   using Ctx = TileCtx<TQ, TV, TO, TC>;
   using V2 = typename Pair2<TC>::type;
@@ -509,6 +523,13 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
   TC* sL = reinterpret_cast<TC*>(smem_raw + NS * P::SLOT + P::FACE);
   uint64_t* bars =
       reinterpret_cast<uint64_t*>(smem_raw + NS * P::SLOT + P::FACE + P::LIFTB);
+  // Tensor-core operands (TCG): A for x and y, hi and lo; B hi and lo; the
+  // MMA barrier and the TMEM address.
+  unsigned char* tcg = smem_raw + NS * P::SLOT + P::FACE + P::LIFTB + P::BARS;
+  unsigned char* tA = tcg;                                      // [xhi, xlo, yhi, ylo]
+  unsigned char* tB = tcg + 4 * tc::kOperandBytes;              // [hi, lo]
+  uint64_t* mma_bar = reinterpret_cast<uint64_t*>(tB + 2 * tc::kBBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tB + 2 * tc::kBBytes + 16);
 
   const int s = threadIdx.x / NQ2;               // element slot of the tile
   const int t = threadIdx.x - s * NQ2;           // column index a + NQ*b
@@ -562,7 +583,22 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
 
   if (threadIdx.x == 0) {
     for (int k = 0; k < NS; ++k) mbar_init(&bars[k], 1);
+    if constexpr (TCG) mbar_init(mma_bar, 1);
     fence_barrier_init();
+  }
+  uint32_t tmem = 0;
+  if constexpr (TCG) {
+    if (threadIdx.x < 32) tc::tmem_alloc(tmem_slot);
+    // B(l, i) = D(i, l), row i, K index l; hi and lo TF32 halves.
+    if (threadIdx.x < 64) {
+      const int i = threadIdx.x >> 3, l = threadIdx.x & 7;
+      const float d = D.d[i * NQ + l];
+      const float hi = tc::to_tf32(d);
+      *reinterpret_cast<float*>(tB + tc::offset(i, l)) = hi;
+      *reinterpret_cast<float*>(tB + tc::kBBytes + tc::offset(i, l)) = tc::to_tf32(d - hi);
+    }
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
   }
   // Factored lift of the fast kernels: l_f(n) is the factored table's entry
   // at normal index n, tangential indices 0 (faces 1, 3 lie along j, faces
@@ -574,6 +610,10 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     }
   }
   __syncthreads();
+  if constexpr (TCG) {
+    tc::fence_after_sync();
+    tmem = *tmem_slot;
+  }
   if (threadIdx.x == 0)
     for (int k = 0; k < NS; ++k) {
       const int tile = blockIdx.x + k * gridDim.x;
@@ -609,6 +649,11 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
           if (tk < ntiles && (T < NS || T - NS + 1 <= it - 1))
             mbar_wait_bounded(&bars[T % NS], (T / NS) & 1, A.wait_spins);
         }
+      }
+      if constexpr (TCG) {
+        // No MMA is in flight (the previous tile's results were read).
+        __syncwarp();
+        if (threadIdx.x < 32) tc::tmem_dealloc(tmem);
       }
       return;
     }
@@ -703,6 +748,17 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         fx[k] = AR::mul(qv, uv);
         fy[k] = AR::mul(qv, vv);
         sz[n] = AR::mul(qv, wv);
+        if constexpr (TCG) {
+          // x line (j, k, e) = (b, k, s) is row m of A_x with K index a; y
+          // line (i, k, e) = (a, k, s) is row m of A_y with K index b.
+          const uint32_t ox = tc::offset(b + 8 * k + 64 * s, a);
+          const uint32_t oy = tc::offset(a + 8 * k + 64 * s, b);
+          const float xh = tc::to_tf32(fx[k]), yh = tc::to_tf32(fy[k]);
+          *reinterpret_cast<float*>(tA + ox) = xh;
+          *reinterpret_cast<float*>(tA + tc::kOperandBytes + ox) = tc::to_tf32(fx[k] - xh);
+          *reinterpret_cast<float*>(tA + 2 * tc::kOperandBytes + oy) = yh;
+          *reinterpret_cast<float*>(tA + 3 * tc::kOperandBytes + oy) = tc::to_tf32(fy[k] - yh);
+        }
         if constexpr (XSPLIT) {
           if (k == 0) qlo = qv;
           if (k == NQ - 1) qhi = qv;
@@ -716,9 +772,28 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         if (ony) fmy[NQ * k] = V2{qv, vv};
       }
     }
+    if constexpr (TCG) fence_proxy_async_smem();  // A operands -> tensor cores
     __syncthreads();   // the slot's u, v are dead: reuse them as line buffers
+    if constexpr (TCG) {
+      if (threadIdx.x == 0) {
+        tc::fence_after_sync();
+        const uint64_t bh = tc::smem_desc(tB), bl = tc::smem_desc(tB + tc::kBBytes);
+#pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          const uint32_t acc = tmem + 8 * d;  // columns 0-7: x, 8-15: y
+          const uint64_t ah = tc::smem_desc(tA + 2 * d * tc::kOperandBytes);
+          const uint64_t al = tc::smem_desc(tA + (2 * d + 1) * tc::kOperandBytes);
+          tc::mma_tf32(acc, ah, bh, false);
+          tc::mma_tf32(acc, al, bh, true);
+          tc::mma_tf32(acc, ah, bl, true);
+        }
+        tc::commit(mma_bar);
+      }
+    }
     if (active) {
-      if constexpr (TENSOR) {
+      if constexpr (TCG) {
+        // The lines come from the tensor cores; no column writes.
+      } else if constexpr (TENSOR) {
         TC* px = sX + TensorIdx8::px(a, b);
         TC* py = sY + TensorIdx8::py(a, b);
 #pragma unroll
@@ -773,7 +848,24 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     TC f5 = TC(0), f6 = TC(0);
     if (active) {
       // ---- Phase 3: x-line and y-line contractions, in place --------------
-      if constexpr (TENSOR) {
+      if constexpr (TCG) {
+        // Wait for this tile's MMAs (bounded), then each thread reads its
+        // x line and y line (TMEM lane = thread) into the line buffers.
+        const bool done = mbar_wait_bounded(mma_bar, it & 1, A.wait_spins);
+        if (!done) atomicExch(A.status, kStatusWaitTimeout);
+        tc::fence_after_sync();
+        float rx[8], ry[8];
+        const uint32_t lane = tmem + (static_cast<uint32_t>(threadIdx.x & ~31) << 16);
+        tc::ld8(lane, rx);
+        tc::ld8(lane + 8, ry);
+        tc::fence_before_sync();
+        const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) {
+          sX[LI::xl(lbx, i)] = rx[i];
+          sY[LI::yl(lby, i)] = ry[i];
+        }
+      } else if constexpr (TENSOR) {
         // DMMA tiles: the element's two warps take four k-planes each; a
         // plane is read and rewritten only by its warp.
         const int lane = threadIdx.x & 31, g = lane >> 2, qd = lane & 3;
@@ -938,6 +1030,11 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
         }
       }
     }
+  }
+  if constexpr (TCG) {
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) tc::tmem_dealloc(tmem);
   }
 }
 

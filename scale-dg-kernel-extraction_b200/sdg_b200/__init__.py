@@ -47,6 +47,7 @@ FIELD_Q, FIELD_U, FIELD_V, FIELD_W = 0, 1, 2, 3
 ARRAY_STAGE2, ARRAY_STAGE3 = 4, 5
 
 VARIANT_AUTO, VARIANT_BLOCK, VARIANT_PIPE, VARIANT_BLOCK8, VARIANT_SPLIT = 0, 1, 2, 3, 4
+VARIANT_TENSOR = 5
 
 # Exported symbols and their signatures (must match include/sdg_gpu.h).
 _I, _D, _P, _LL = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong

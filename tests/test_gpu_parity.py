@@ -266,3 +266,40 @@ def test_fast_high_order_variants_agree(p):
     qo = q.copy(order="F")
     orc.run_rk3(orc.OPT1, qo, u, v, w, ops, omesh, dt, nstep)
     assert rel_maxnorm(res[1], qo[:, : mesh.Ne]) <= TOL
+
+
+def test_mixed_tensor_core_lines():
+    """Kernel variant 5: the mixed form's x/y lines at p = 7 on the tensor
+    cores (TF32, three hi/lo passes, TMEM accumulators).  Its rounding
+    differs from the FP32 FMA lines, so it is checked against the FP64
+    oracle with the mixed form's bar; at other orders the variant falls back
+    to the automatic one (same bits)."""
+    p, dims, nstep = 7, (4, 4, 4), 50
+    ops, mesh, omesh, (q, u, v, w) = case(p, dims)
+    dt = 0.1 / 4 / (p + 1) ** 2
+    res = {}
+    for var in (sdg.VARIANT_AUTO, sdg.VARIANT_TENSOR):
+        h = sdg.Handle(ops, mesh, sdg.FLAG_MIXED)
+        h.set_kernel_variant(var)
+        h.set_state(q, u, v, w)
+        h.rk3_steps(dt, nstep)
+        res[var] = h.get_field()
+        h.close()
+    qo = q.copy(order="F")
+    orc.run_rk3(orc.OPT1, qo, u, v, w, ops, omesh, dt, nstep)
+    ref = qo[:, : mesh.Ne]
+    for var, got in res.items():
+        err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert err <= 1e-5, (var, err)
+    assert not np.array_equal(res[sdg.VARIANT_AUTO], res[sdg.VARIANT_TENSOR])
+    # another order: the variant runs the automatic kernel
+    ops, mesh, omesh, (q, u, v, w) = case(5, (3, 3, 2))
+    out = []
+    for var in (sdg.VARIANT_AUTO, sdg.VARIANT_TENSOR):
+        h = sdg.Handle(ops, mesh, sdg.FLAG_MIXED)
+        h.set_kernel_variant(var)
+        h.set_state(q, u, v, w)
+        h.rk3_steps(0.1 / 3 / 36, 5)
+        out.append(h.get_field())
+        h.close()
+    assert np.array_equal(out[0], out[1])
