@@ -812,7 +812,9 @@ struct sdg_server {
   std::condition_variable cv;      // worker: uploaded requests, stop
   std::condition_variable up_cv;   // uploader: a request queued, memory freed, stop
   std::condition_variable done_cv; // a request finished
+  std::condition_variable ret_cv;  // retirer: finished requests to copy out
   std::deque<Inst*> queue;
+  std::vector<Inst*> to_retire;    // finished, waiting for the retirer
   std::vector<Inst*> active;       // members of the running chunk's graph
   std::vector<Inst*> joining;      // uploaded, joining at the next chunk
   int uploading = 0;               // admitted, upload in progress
@@ -825,7 +827,7 @@ struct sdg_server {
   bool stop = false;
   int error = SDG_OK;
   std::string error_msg;
-  std::thread worker, uploader;
+  std::thread worker, uploader, retirer;
   double busy = 0;            // seconds of device time of the chunks
   long long dof_steps = 0;    // DOF x RK steps completed
   long long steps_run = 0;    // RK steps run (over all chunks)
@@ -882,6 +884,26 @@ struct sdg_server {
       // chunk runs.
       std::vector<Inst*> done = finish_chunk();
       launch_chunk();
+      if (!done.empty()) {
+        std::lock_guard<std::mutex> lk(mu);
+        to_retire.insert(to_retire.end(), done.begin(), done.end());
+        ret_cv.notify_all();
+      }
+    }
+  }
+
+  // Copies finished requests' results to the host and returns their memory,
+  // so that neither the worker nor the GPU waits for those copies.
+  void retire_loop() {
+    cudaSetDevice(ens.dev);
+    for (;;) {
+      std::vector<Inst*> done;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        ret_cv.wait(lk, [&] { return stop || !to_retire.empty(); });
+        if (stop) return;
+        done.swap(to_retire);
+      }
       retire(done);
     }
   }
@@ -1023,7 +1045,9 @@ std::vector<Inst*> sdg_server::finish_chunk() {
 }
 
 // Copies the finished members' results to the host on the output stream and
-// returns their memory; the running chunk no longer touches them.
+// returns their memory; the running chunks no longer touch them.  The pool
+// free is ordered after the copy on the same stream, and Ensemble::release
+// touches no shared tables.
 void sdg_server::retire(std::vector<Inst*>& done) {
   if (done.empty()) return;
   for (Inst* I : done) {
@@ -1128,6 +1152,7 @@ int sdg_serve_create(sdg_server** out, double max_bytes) {
   sdg_server* raw = s.release();
   raw->worker = std::thread([raw] { raw->loop(); });
   raw->uploader = std::thread([raw] { raw->upload_loop(); });
+  raw->retirer = std::thread([raw] { raw->retire_loop(); });
   *out = raw;
   return SDG_OK;
 }
@@ -1227,14 +1252,17 @@ int sdg_serve_destroy(sdg_server* s) {
     s->stop = true;
     s->cv.notify_all();
     s->up_cv.notify_all();
+    s->ret_cv.notify_all();
   }
   if (s->worker.joinable()) s->worker.join();
   if (s->uploader.joinable()) s->uploader.join();
+  if (s->retirer.joinable()) s->retirer.join();
   cudaSetDevice(s->ens.dev);
   cudaStreamSynchronize(s->ens.stream);
   cudaStreamSynchronize(s->up_stream);
   for (Inst* I : s->active) s->ens.release(I, s->ens.stream);
   for (Inst* I : s->joining) s->ens.release(I, s->ens.stream);
+  for (Inst* I : s->to_retire) s->ens.release(I, s->ens.stream);
   cudaStreamSynchronize(s->ens.stream);
   delete s;
   return SDG_OK;

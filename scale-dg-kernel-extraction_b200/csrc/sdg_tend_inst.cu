@@ -25,8 +25,12 @@ constexpr int NQ = SDG_NQ;
 // kernel is a template argument so that the set-up state belongs to that
 // kernel: kernels of one signature (tendency and stage forms) differ in
 // their shared-memory plans.
+// floor_blocks: resident blocks per SM to launch at least (the occupancy
+// query reports one block per SM for kernels that allocate tensor memory,
+// whose shared memory, registers and 32 TMEM columns allow more).
 template <auto KERN, int THREADS = PipeGeo<NQ>::THREADS, typename Args, typename Dm>
-int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, const Dm& d) {
+int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, const Dm& d,
+                int floor_blocks = 0) {
   constexpr auto kern = KERN;
   static DeviceSetup setup;  // blocks per SM, per kernel and device
   const int dev = setup_device();
@@ -40,7 +44,7 @@ int launch_pipe(size_t smem, int ntiles, const LaunchSpec& s, const Args& a, con
     int nb = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, THREADS, smem);
     if (e != cudaSuccess) return static_cast<int>(e);
-    blocks_per_sm = nb > 0 ? nb : 1;
+    blocks_per_sm = std::max(nb > 0 ? nb : 1, floor_blocks);
     setup.slot[dev].store(blocks_per_sm, std::memory_order_relaxed);
   }
   if (ntiles <= 0) return 0;
@@ -122,8 +126,11 @@ int run(const LaunchSpec& s) {
     using TP = PipePlan<NQ, TQ, TV, TC, STAGE, true>;
     if (s.variant == kVariantTensor && !batch && can_pipe && TP::BYTES <= device_smem_optin()) {
       const int ntiles = (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
+      // Blocks per SM of the plan and the launch bounds: 4 x 32 TMEM columns
+      // of the SM's 512.
+      constexpr int fb = pipe_min_blocks<NQ, TQ, TV, TC, EXACT, STAGE, true>();
       return launch_pipe<tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false, true>>(
-          TP::BYTES, ntiles, s, a, d);
+          TP::BYTES, ntiles, s, a, d, fb);
     }
   }
   if (batch && !can_pipe) return static_cast<int>(cudaErrorNotSupported);
