@@ -151,7 +151,14 @@ struct Group {
   int epb = 1;
   int variant = kVariantAuto;   // set by the autotuner
   bool dirty = true;
-  BatchInst* d_insts = nullptr;  // [3][inst_cap]
+  // Device tables, two buffers: a rebuild writes the buffer that no launch
+  // still in flight reads (at most two chunks of steps are in flight in the
+  // serving loop) and makes it current.
+  BatchInst* d_insts_buf[2] = {nullptr, nullptr};  // [3][inst_cap]
+  BatchTile* d_tiles_buf[2] = {nullptr, nullptr};
+  int inst_cap_buf[2] = {0, 0}, tile_cap_buf[2] = {0, 0};
+  int cur = 0;
+  BatchInst* d_insts = nullptr;  // the current buffer
   BatchTile* d_tiles = nullptr;
   int inst_cap = 0, tile_cap = 0, ntiles = 0;
   std::vector<BatchInst> h_insts;
@@ -177,8 +184,10 @@ struct Ensemble {
     cudaSetDevice(dev);
     if (stream) cudaStreamSynchronize(stream);
     for (auto& g : groups) {
-      if (g.second->d_insts) cudaFree(g.second->d_insts);
-      if (g.second->d_tiles) cudaFree(g.second->d_tiles);
+      for (int b = 0; b < 2; ++b) {
+        if (g.second->d_insts_buf[b]) cudaFree(g.second->d_insts_buf[b]);
+        if (g.second->d_tiles_buf[b]) cudaFree(g.second->d_tiles_buf[b]);
+      }
       if (g.second->stream) cudaStreamDestroy(g.second->stream);
       if (g.second->done) cudaEventDestroy(g.second->done);
     }
@@ -385,16 +394,23 @@ struct Ensemble {
         g->h_tiles.push_back(BatchTile{m, e0, std::min(g->epb, I->ne - e0), 0});
     }
     g->ntiles = static_cast<int>(g->h_tiles.size());
-    if (3 * ni > 3 * g->inst_cap) {
-      if (g->d_insts) cudaFree(g->d_insts);
-      g->inst_cap = std::max(ni, 2 * g->inst_cap);
-      ENS_CUDA(cudaMalloc(&g->d_insts, 3L * g->inst_cap * sizeof(BatchInst)));
+    const int b = g->cur ^ 1;  // the buffer no launch in flight reads
+    if (ni > g->inst_cap_buf[b]) {
+      if (g->d_insts_buf[b]) cudaFree(g->d_insts_buf[b]);
+      g->inst_cap_buf[b] = std::max(ni, 2 * g->inst_cap_buf[b]);
+      ENS_CUDA(cudaMalloc(&g->d_insts_buf[b], 3L * g->inst_cap_buf[b] * sizeof(BatchInst)));
     }
-    if (g->ntiles > g->tile_cap) {
-      if (g->d_tiles) cudaFree(g->d_tiles);
-      g->tile_cap = std::max(g->ntiles, 2 * g->tile_cap);
-      ENS_CUDA(cudaMalloc(&g->d_tiles, static_cast<size_t>(g->tile_cap) * sizeof(BatchTile)));
+    if (g->ntiles > g->tile_cap_buf[b]) {
+      if (g->d_tiles_buf[b]) cudaFree(g->d_tiles_buf[b]);
+      g->tile_cap_buf[b] = std::max(g->ntiles, 2 * g->tile_cap_buf[b]);
+      ENS_CUDA(cudaMalloc(&g->d_tiles_buf[b],
+                          static_cast<size_t>(g->tile_cap_buf[b]) * sizeof(BatchTile)));
     }
+    g->cur = b;
+    g->d_insts = g->d_insts_buf[b];
+    g->d_tiles = g->d_tiles_buf[b];
+    g->inst_cap = g->inst_cap_buf[b];
+    g->tile_cap = g->tile_cap_buf[b];
     if (ni > 0) {
       // Instance tables are laid out [stage][inst_cap]; pad each stage.
       std::vector<BatchInst> padded(3L * g->inst_cap);
@@ -780,21 +796,22 @@ int sdg_batch_destroy(sdg_batch* b) {
 // ===========================================================================
 // Serving loop
 // ===========================================================================
-// Two threads own the GPU side.  The uploader admits queued requests in
+// Three threads own the GPU side.  The uploader admits queued requests in
 // arrival order while their device memory fits under the byte cap and
-// uploads each on a stream of its own, so neither the running chunk nor the
-// worker waits for host-to-device copies.  The worker advances the admitted
-// requests in chunks of RK steps.  Each chunk replays the CUDA graph of one
-// RK step of the current membership (all orders and sizes in one fork/join
-// of batched launches) n times, n = min(steps that fit in about kChunkMs of
-// device time, the fewest steps any member has left), so no member overruns
-// and the host meets the GPU once per chunk, not once per step.  At the
-// chunk boundary the worker reads the status word of the bounded waits once,
-// copies out the results of the members that chunk finished (on a third
-// stream) and returns their memory, lets the uploaded requests join,
-// re-captures the step graph if the membership changed, and launches the
-// next chunk.  Requests that arrive while others run join at the next chunk
-// boundary, so their work overlaps the others' on the device.
+// uploads each on a stream of its own, so neither the GPU nor the worker
+// waits for host-to-device copies.  The worker advances the admitted requests
+// in chunks of RK steps: one chunk enqueues n RK steps of the current
+// membership (every order and precision in one fork/join of batched launches
+// per step), n = min(steps that fit in about kChunkMs of device time, the
+// fewest steps any member has left), so no member overruns.  Up to two
+// chunks are in flight: the worker enqueues the next chunk before it waits
+// for the oldest, so the GPU does not idle while the host turns around.  A
+// member whose steps end with a chunk leaves the membership when that chunk
+// is enqueued; once the chunk completes (its status word checked), the
+// retirer copies the results out on a stream of its own and returns the
+// memory.  Requests uploaded meanwhile join the next chunk.  Membership
+// changes rewrite a group's tile tables into the table buffer that no chunk
+// in flight reads (Group keeps two).
 constexpr int kChunkSteps = 16;
 constexpr double kChunkMs = 8.0;
 
@@ -838,17 +855,25 @@ struct sdg_server {
 
   // Worker-only state.
   cudaStream_t up_stream = nullptr;  // uploads (uploader thread)
-  cudaStream_t out_stream = nullptr; // result downloads (worker)
-  cudaGraphExec_t graph = nullptr;   // one RK step of `active`
-  bool graph_stale = true;
-  cudaEvent_t c0 = nullptr, c1 = nullptr;  // brackets of the running chunk
-  int chunk_steps = 0;
+  cudaStream_t out_stream = nullptr; // result downloads (retirer thread)
+  // A chunk in flight: its events, steps, DOF per step and the members whose
+  // steps end with it.
+  struct Chunk {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int steps = 0;
+    long long dof = 0;
+    std::vector<Inst*> finishing;
+  };
+  Chunk chunk[2];
+  int oldest = 0;                    // ring position of the oldest chunk
+  int in_flight = 0;                 // chunks enqueued, not yet completed
   double step_ms = 0;                // device time per step of the last chunk
 
   ~sdg_server() {
-    if (graph) cudaGraphExecDestroy(graph);
-    if (c0) cudaEventDestroy(c0);
-    if (c1) cudaEventDestroy(c1);
+    for (auto& c : chunk) {
+      if (c.e0) cudaEventDestroy(c.e0);
+      if (c.e1) cudaEventDestroy(c.e1);
+    }
     if (up_stream) cudaStreamDestroy(up_stream);
     if (out_stream) cudaStreamDestroy(out_stream);
   }
@@ -856,8 +881,10 @@ struct sdg_server {
   int init_worker_state() {
     ENS_CUDA(cudaStreamCreateWithFlags(&up_stream, cudaStreamNonBlocking));
     ENS_CUDA(cudaStreamCreateWithFlags(&out_stream, cudaStreamNonBlocking));
-    ENS_CUDA(cudaEventCreate(&c0));
-    ENS_CUDA(cudaEventCreate(&c1));
+    for (auto& c : chunk) {
+      ENS_CUDA(cudaEventCreate(&c.e0));
+      ENS_CUDA(cudaEventCreate(&c.e1));
+    }
     return SDG_OK;
   }
 
@@ -874,21 +901,17 @@ struct sdg_server {
       {
         std::unique_lock<std::mutex> lk(mu);
         cv.wait(lk, [&] {
-          return stop || !active.empty() || !joining.empty() || chunk_running;
+          return stop || !active.empty() || !joining.empty() || in_flight > 0;
         });
         if (stop) return;
       }
       // Only the worker changes the membership and launches; the uploader
-      // only adds operators and groups (under ens_mu) and uploads.  The
-      // results of the finished members are copied out while the next
-      // chunk runs.
-      std::vector<Inst*> done = finish_chunk();
-      launch_chunk();
-      if (!done.empty()) {
-        std::lock_guard<std::mutex> lk(mu);
-        to_retire.insert(to_retire.end(), done.begin(), done.end());
-        ret_cv.notify_all();
-      }
+      // only adds operators and groups (under ens_mu) and uploads.
+      join_uploaded();
+      if (!active.empty() && in_flight < 2) launch_chunk();
+      // Complete the oldest chunk once the next one is queued (or nothing
+      // else can be queued).
+      if (in_flight == 2 || (in_flight == 1 && active.empty())) complete_oldest();
     }
   }
 
@@ -909,8 +932,9 @@ struct sdg_server {
   }
 
   void fail_all(int rc);
-  std::vector<Inst*> finish_chunk();
+  void join_uploaded();
   void launch_chunk();
+  void complete_oldest();
   void retire(std::vector<Inst*>& done);
 };
 
@@ -966,6 +990,7 @@ void sdg_server::upload_loop() {
 // Fails every request on the device after an error (the worker keeps
 // serving later submissions).
 void sdg_server::fail_all(int rc) {
+  cudaStreamSynchronize(ens.stream);
   std::lock_guard<std::mutex> el(ens_mu);
   std::lock_guard<std::mutex> lk(mu);
   error = rc;
@@ -977,71 +1002,114 @@ void sdg_server::fail_all(int rc) {
       used -= I->bytes;
       I->state = kFailed;
     }
+  for (auto& c : chunk) {
+    for (Inst* I : c.finishing) {
+      ens.release(I, out_stream);
+      used -= I->bytes;
+      I->state = kFailed;
+    }
+    retiring -= static_cast<int>(c.finishing.size());
+    c.finishing.clear();
+  }
   active.clear();
   joining.clear();
+  in_flight = 0;
   chunk_running = false;
-  graph_stale = true;
   up_cv.notify_all();
   done_cv.notify_all();
 }
 
-// Waits for the running chunk, accounts it, takes the members it finished
-// out of their groups (returned, for retire) and lets the uploaded requests
-// join.
-std::vector<Inst*> sdg_server::finish_chunk() {
-  std::vector<Inst*> done;
-  if (chunk_running) {
-    cudaError_t ce = cudaEventSynchronize(c1);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c0, c1);
-    int rc = ce == cudaSuccess ? SDG_OK
-                               : fail(SDG_ERR_CUDA, "serving chunk failed: %s",
-                                      cudaGetErrorString(ce));
-    if (!rc) rc = ens.check_status();
-    if (chunk_steps > 0) step_ms = ms / chunk_steps;
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      busy += 1e-3 * ms;
-      steps_run += chunk_steps;
-      ++chunks;
-    }
-    if (rc) {
-      fail_all(rc);
-      return done;
-    }
-    std::vector<Inst*> keep;
-    long long dof = 0;
-    for (Inst* I : active) {
-      dof += static_cast<long long>(I->np) * I->ne;
-      I->steps_left -= chunk_steps;
-      (I->steps_left > 0 ? keep : done).push_back(I);
-    }
-    {
-      std::lock_guard<std::mutex> el(ens_mu);
-      for (Inst* I : done) {
-        ens.leave(I);
-        graph_stale = true;
-      }
-    }
-    std::lock_guard<std::mutex> lk(mu);  // `active` is read by sdg_serve_wait
-    active.swap(keep);
-    retiring += static_cast<int>(done.size());
-    dof_steps += dof * chunk_steps;
-    chunk_running = false;
-  }
+// Lets the uploaded requests join the membership of the next chunk.
+void sdg_server::join_uploaded() {
   std::vector<Inst*> join;
   {
     std::lock_guard<std::mutex> lk(mu);
     join.swap(joining);
   }
-  if (!join.empty()) {
-    std::lock_guard<std::mutex> el(ens_mu);
-    for (Inst* I : join) ens.join(I, ens.groups.at(std::make_pair(I->nq, I->mixed)).get());
-    graph_stale = true;
+  if (join.empty()) return;
+  std::lock_guard<std::mutex> el(ens_mu);
+  for (Inst* I : join) ens.join(I, ens.groups.at(std::make_pair(I->nq, I->mixed)).get());
+  std::lock_guard<std::mutex> lk(mu);
+  active.insert(active.end(), join.begin(), join.end());
+}
+
+// Waits for the oldest chunk in flight, accounts it, checks the status word
+// and hands the members it finished to the retirer.
+void sdg_server::complete_oldest() {
+  Chunk& c = chunk[oldest];
+  cudaError_t ce = cudaEventSynchronize(c.e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c.e0, c.e1);
+  int rc = ce == cudaSuccess ? SDG_OK
+                             : fail(SDG_ERR_CUDA, "serving chunk failed: %s",
+                                    cudaGetErrorString(ce));
+  if (!rc) rc = ens.check_status();
+  if (c.steps > 0) step_ms = ms / c.steps;
+  std::vector<Inst*> done;
+  done.swap(c.finishing);
+  {
     std::lock_guard<std::mutex> lk(mu);
-    active.insert(active.end(), join.begin(), join.end());
+    busy += 1e-3 * ms;
+    steps_run += c.steps;
+    dof_steps += c.dof * c.steps;
+    ++chunks;
+    --in_flight;
+    oldest ^= 1;
+    if (!rc) {
+      to_retire.insert(to_retire.end(), done.begin(), done.end());
+      ret_cv.notify_all();
+    }
+    chunk_running = in_flight > 0;
   }
-  return done;
+  if (rc) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      chunk[oldest ^ 1].finishing.swap(done);  // fail these with the rest
+    }
+    fail_all(rc);
+  }
+}
+
+// Enqueues the next chunk: n RK steps of the current membership.  Members
+// whose steps end with it leave the membership now (their results are final
+// once the chunk completes).
+void sdg_server::launch_chunk() {
+  long long n = kChunkSteps;
+  if (step_ms > 0) n = std::max(1LL, std::min(n, static_cast<long long>(kChunkMs / step_ms)));
+  for (Inst* I : active) n = std::min(n, I->steps_left);
+  Chunk& c = chunk[oldest ^ in_flight];
+  c.steps = static_cast<int>(n);
+  c.dof = 0;
+  c.finishing.clear();
+  int rc = SDG_OK;
+  {
+    std::lock_guard<std::mutex> el(ens_mu);
+    // Tables of changed groups (into the buffer no chunk in flight reads)
+    // and the kernels' one-time set-up.
+    rc = ens.prime();
+    cudaEventRecord(c.e0, ens.stream);
+    for (int k = 0; k < c.steps && !rc; ++k) rc = ens.step(ens.stream);
+    cudaEventRecord(c.e1, ens.stream);
+  }
+  if (rc) {
+    fail_all(rc);
+    return;
+  }
+  std::vector<Inst*> keep;
+  for (Inst* I : active) {
+    c.dof += static_cast<long long>(I->np) * I->ne;
+    I->steps_left -= n;
+    (I->steps_left > 0 ? keep : c.finishing).push_back(I);
+  }
+  if (!c.finishing.empty()) {
+    std::lock_guard<std::mutex> el(ens_mu);
+    for (Inst* I : c.finishing) ens.leave(I);
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  active.swap(keep);
+  retiring += static_cast<int>(c.finishing.size());
+  ++in_flight;
+  chunk_running = true;
 }
 
 // Copies the finished members' results to the host on the output stream and
@@ -1066,73 +1134,6 @@ void sdg_server::retire(std::vector<Inst*>& done) {
   retiring -= static_cast<int>(done.size());
   up_cv.notify_all();
   done_cv.notify_all();
-}
-
-// Re-captures the step graph if the membership changed and launches the
-// next chunk: as many steps as fit in about kChunkMs of device time at the
-// last measured step time (at most kChunkSteps, at least one), so that a
-// request that arrives meanwhile waits at most about that long to join.
-void sdg_server::launch_chunk() {
-  if (active.empty()) {
-    if (graph) {
-      cudaGraphExecDestroy(graph);
-      graph = nullptr;
-    }
-    return;
-  }
-  int rc = SDG_OK;
-  std::unique_lock<std::mutex> el(ens_mu);
-  if (graph_stale) {
-    if (graph) {
-      cudaGraphExecDestroy(graph);
-      graph = nullptr;
-    }
-    // Tables and the kernels' one-time set-up outside the capture.
-    rc = ens.prime();
-    cudaGraph_t gr = nullptr;
-    if (!rc) {
-      cudaError_t e = cudaStreamBeginCapture(ens.stream, cudaStreamCaptureModeThreadLocal);
-      if (e != cudaSuccess) {
-        rc = fail(SDG_ERR_CUDA, "serving graph capture: %s", cudaGetErrorString(e));
-      } else {
-        rc = ens.step(ens.stream);
-        e = cudaStreamEndCapture(ens.stream, &gr);
-        if (!rc && e != cudaSuccess)
-          rc = fail(SDG_ERR_CUDA, "serving graph capture: %s", cudaGetErrorString(e));
-      }
-    }
-    if (!rc) {
-      cudaError_t e = cudaGraphInstantiate(&graph, gr, 0);
-      if (e != cudaSuccess)
-        rc = fail(SDG_ERR_CUDA, "serving graph instantiate: %s", cudaGetErrorString(e));
-    }
-    if (gr) cudaGraphDestroy(gr);
-    if (rc) {
-      el.unlock();
-      fail_all(rc);
-      return;
-    }
-    graph_stale = false;
-  }
-  el.unlock();
-  long long n = kChunkSteps;
-  if (step_ms > 0) n = std::max(1LL, std::min(n, static_cast<long long>(kChunkMs / step_ms)));
-  for (Inst* I : active) n = std::min(n, I->steps_left);
-  chunk_steps = static_cast<int>(n);
-  cudaEventRecord(c0, ens.stream);
-  for (int k = 0; k < chunk_steps && !rc; ++k) {
-    cudaError_t e = cudaGraphLaunch(graph, ens.stream);
-    if (e != cudaSuccess)
-      rc = fail(SDG_ERR_CUDA, "serving graph launch: %s", cudaGetErrorString(e));
-  }
-  cudaEventRecord(c1, ens.stream);
-  if (rc) {
-    cudaStreamSynchronize(ens.stream);
-    fail_all(rc);
-    return;
-  }
-  std::lock_guard<std::mutex> lk(mu);
-  chunk_running = true;
 }
 
 extern "C" {
