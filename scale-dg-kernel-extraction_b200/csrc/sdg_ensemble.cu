@@ -832,7 +832,7 @@ struct sdg_server {
   std::condition_variable ret_cv;  // retirer: finished requests to copy out
   std::deque<Inst*> queue;
   std::vector<Inst*> to_retire;    // finished, waiting for the retirer
-  std::vector<Inst*> active;       // members of the running chunk's graph
+  std::vector<Inst*> active;       // members of the next chunk
   std::vector<Inst*> joining;      // uploaded, joining at the next chunk
   int uploading = 0;               // admitted, upload in progress
   int retiring = 0;                // finished, results being copied out
@@ -1264,6 +1264,8 @@ int sdg_serve_destroy(sdg_server* s) {
   for (Inst* I : s->active) s->ens.release(I, s->ens.stream);
   for (Inst* I : s->joining) s->ens.release(I, s->ens.stream);
   for (Inst* I : s->to_retire) s->ens.release(I, s->ens.stream);
+  for (auto& c : s->chunk)
+    for (Inst* I : c.finishing) s->ens.release(I, s->ens.stream);
   cudaStreamSynchronize(s->ens.stream);
   delete s;
   return SDG_OK;
