@@ -86,12 +86,14 @@ int run(const LaunchSpec& s) {
   for (int i = 0; i < 2 * NQ; ++i)
     d.lz[i] = s.lift_z ? static_cast<TC>(s.lift_z[i]) : TC(0);
   using P = PipePlan<NQ, TQ, TV, TC, STAGE>;
+  using PB = PipePlan<NQ, TQ, TV, TC, STAGE, false, true>;  // batched launches
   auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
   const bool batch = s.batch_tiles != nullptr;
   // Batched arrays are allocated 256-byte aligned by the batch itself.  The
   // fast pipelined kernels need the factored lift; with a verbatim table a
   // fast launch takes the one-tile-per-block kernel.
-  const bool can_pipe = P::BYTES <= kPipeMaxSmem && P::BYTES <= device_smem_optin() &&
+  const size_t pipe_bytes = batch ? PB::BYTES : P::BYTES;
+  const bool can_pipe = pipe_bytes <= kPipeMaxSmem && pipe_bytes <= device_smem_optin() &&
                         (EXACT || s.lift_z != nullptr) &&
                         (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
                                    aligned(s.w) && aligned(s.escale) && aligned(s.fscale)));
@@ -142,7 +144,7 @@ int run(const LaunchSpec& s) {
         batch ? s.batch_ntiles : (s.nelem + PipeGeo<NQ>::EPB - 1) / PipeGeo<NQ>::EPB;
     if (batch)
       return launch_pipe<tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, true>>(
-          P::BYTES, ntiles, s, a, d);
+          PB::BYTES, ntiles, s, a, d);
     return launch_pipe<tend_pipe_kernel<NQ, TQ, TV, TO, TC, EXACT, ORDER, STAGE, false>>(
         P::BYTES, ntiles, s, a, d);
   }
@@ -208,7 +210,8 @@ int run(const LaunchSpec& s) {
 template <typename TQ, typename TV, typename TC, bool STAGE>
 int pipe_fits() {
   const size_t optin = device_smem_optin();
-  constexpr size_t bytes = PipePlan<NQ, TQ, TV, TC, STAGE>::BYTES;
+  // Batched plans (the ensemble asks): the tile context travels in the slot.
+  constexpr size_t bytes = PipePlan<NQ, TQ, TV, TC, STAGE, false, true>::BYTES;
   int r = (bytes <= kPipeMaxSmem && bytes <= optin) ? 1 : 0;
   if constexpr (NQ >= 9) {
     constexpr size_t sb = SplitPlan<NQ, kSplitH<NQ>, TQ, TV, TC, STAGE>::BYTES;

@@ -340,7 +340,10 @@ struct PipeGeo {
 // Shared-memory plan of the pipelined kernel.  TCG adds the operands of the
 // tensor-core line contractions (sdg_tcgen05.cuh): x and y, hi and lo, the
 // hi and lo halves of D, the TMEM address and the MMA completion barrier.
-template <int NQ, typename TQ, typename TV, typename TC, bool STAGE, bool TCG = false>
+// BATCH adds to each slot the tile's face-neighbour rows and its TileCtx
+// (instance pointers, first element, count), written by the producer.
+template <int NQ, typename TQ, typename TV, typename TC, bool STAGE, bool TCG = false,
+          bool BATCH = false>
 struct PipePlan {
   using G = PipeGeo<NQ>;
   static constexpr int EPB = G::EPB;
@@ -358,12 +361,16 @@ struct PipePlan {
          r16(sizeof(TC) * EPB * LineIdx<NQ, static_cast<int>(sizeof(TC))>::SIZE));
   static constexpr size_t EB = r16(sizeof(TC) * 3 * EPB + 32);  // escale rows
   static constexpr size_t FB = r16(sizeof(TC) * 6 * EPB + 32);  // fscale rows
+  static constexpr size_t PB = BATCH ? r16(sizeof(int) * 6 * EPB + 32) : 0;  // pbase rows
+  static constexpr size_t CB = BATCH ? 128 : 0;                   // TileCtx
   static constexpr size_t OFF_U = QB;
   static constexpr size_t OFF_V = QB + VB;
   static constexpr size_t OFF_W = QB + 2 * VB;
   static constexpr size_t OFF_E = QB + 3 * VB;
   static constexpr size_t OFF_F = OFF_E + EB;
-  static constexpr size_t SLOT = OFF_F + FB;
+  static constexpr size_t OFF_P = OFF_F + FB;
+  static constexpr size_t OFF_C = OFF_P + PB;
+  static constexpr size_t SLOT = OFF_C + CB;
   // (q, un) pairs of the four x/y faces' minus side, per element.
   static constexpr size_t FACE = r16(sizeof(TC) * FaceArea<NQ, sizeof(TC) == 8>::ELEM * EPB);
   // Per-face lift factors l_f(n) of the fast kernels, (4, Nq).
@@ -478,9 +485,9 @@ __device__ __forceinline__ uint32_t tile_shift(int e0, size_t per_elem) {
 // fast FP64 kernels at Nq = 7 (at the four-block budget of 128 registers they
 // spill 36 bytes; three blocks measured 10 % faster: 62.7 -> 69.1 G).
 template <int NQ, typename TQ, typename TV, typename TC, bool EXACT, bool STAGE,
-          bool TCG = false>
+          bool TCG = false, bool BATCH = false>
 constexpr int pipe_min_blocks() {
-  constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE, TCG>::MIN_BLOCKS;
+  constexpr int m = PipePlan<NQ, TQ, TV, TC, STAGE, TCG, BATCH>::MIN_BLOCKS;
   if constexpr (sizeof(TC) == 8 && !EXACT && NQ == 7) return m > 3 ? 3 : m;
   return ((EXACT || (sizeof(TC) == 8 && NQ >= 9) || NQ >= 12) && m > 2) ? 2 : m;
 }
@@ -498,11 +505,12 @@ constexpr int pipe_min_blocks() {
 template <int NQ, typename TQ, typename TV, typename TO, typename TC, bool EXACT,
           int ORDER, bool STAGE, bool BATCH, bool TCG = false>
 __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
-                                  (pipe_min_blocks<NQ, TQ, TV, TC, EXACT, STAGE, TCG>()))
+                                  (pipe_min_blocks<NQ, TQ, TV, TC, EXACT, STAGE, TCG, BATCH>()))
     tend_pipe_kernel(const __grid_constant__ TendArgs<TQ, TV, TO, TC> A,
                      const __grid_constant__ DMat<NQ, TC> D) {
   using G = PipeGeo<NQ>;
-  using P = PipePlan<NQ, TQ, TV, TC, STAGE, TCG>;
+  using P = PipePlan<NQ, TQ, TV, TC, STAGE, TCG, BATCH>;
+  static_assert(sizeof(TileCtx<TQ, TV, TO, TC>) <= 128, "TileCtx fits its slot area");
   static_assert(!TCG || (NQ == 8 && sizeof(TC) == 4 && !EXACT && G::THREADS == 128),
                 "tensor-core lines: fast FP32 at Nq = 8, 128 threads");
   using AR = Ar<TC, EXACT>;
@@ -555,20 +563,25 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     if (tile + 1 == A.inject_skip) return;
     const Ctx c = tile_ctx<EPB, BATCH>(A, tile, ntiles);
     unsigned char* base = slots + slot * P::SLOT;
-    const void* src[6] = {c.q, c.u, c.v, c.w, c.escale, c.fscale};
-    const size_t per[6] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
-                           sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6};
-    const size_t off[6] = {0, P::OFF_U, P::OFF_V, P::OFF_W, P::OFF_E, P::OFF_F};
-    size_t lo[6];
-    uint32_t by[6], sh[6], total = 0;
+    // Batched tiles: the tile's context goes with it, so that the consumers
+    // read it from shared memory instead of the tile and instance tables.
+    if constexpr (BATCH) *reinterpret_cast<Ctx*>(base + P::OFF_C) = c;
+    constexpr int NB = BATCH ? 7 : 6;  // + the face-neighbour rows
+    const void* src[7] = {c.q, c.u, c.v, c.w, c.escale, c.fscale, c.pbase};
+    const size_t per[7] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
+                           sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6,
+                           sizeof(int) * 6};
+    const size_t off[7] = {0, P::OFF_U, P::OFF_V, P::OFF_W, P::OFF_E, P::OFF_F, P::OFF_P};
+    size_t lo[7];
+    uint32_t by[7], sh[7], total = 0;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < NB; ++k) {
       tile_range(c.e0, c.n, per[k], &lo[k], &by[k], &sh[k]);
       total += by[k];
     }
     mbar_arrive_expect_tx(&bars[slot], total);
 #pragma unroll
-    for (int k = 0; k < 6; ++k)
+    for (int k = 0; k < NB; ++k)
       bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
                &bars[slot]);
     // q0 (RK stages 2-3) is read by the epilogue straight from global
@@ -625,15 +638,21 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
     if (tile >= ntiles) break;
     const int slot = it % NS;
     const uint32_t parity = (it / NS) & 1;
-    const Ctx C = tile_ctx<EPB, BATCH>(A, tile, ntiles);
-    const bool active = s < C.n;
-    const int e = C.e0 + (active ? s : 0);
-    const long base = static_cast<long>(e) * NP;
-
-    // The element's face-neighbour row, needed after phase 1.
+    // A single instance's tile context comes from the parameters; the
+    // element's face-neighbour row, needed after phase 1, is loaded before
+    // the wait.  A batched tile's context and rows come with the tile.
+    Ctx C;
     int pbc[6];
+    bool active = false;
+    int e = 0;
+    if constexpr (!BATCH) {
+      C = tile_ctx<EPB, false>(A, tile, ntiles);
+      active = s < C.n;
+      e = C.e0 + (active ? s : 0);
 #pragma unroll
-    for (int f = 0; f < 6; ++f) pbc[f] = active ? ldro(C.pbase + 6 * static_cast<long>(e) + f) : 0;
+      for (int f = 0; f < 6; ++f)
+        pbc[f] = active ? ldro(C.pbase + 6 * static_cast<long>(e) + f) : 0;
+    }
 
     // ---- Wait for the tile's slot (bounded, block-uniform) -----------------
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity, A.wait_spins));
@@ -657,6 +676,17 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
       }
       return;
     }
+    if constexpr (BATCH) {
+      const unsigned char* sb0 = slots + slot * P::SLOT;
+      C = *reinterpret_cast<const Ctx*>(sb0 + P::OFF_C);
+      active = s < C.n;
+      e = C.e0 + (active ? s : 0);
+      const int* spb =
+          reinterpret_cast<const int*>(sb0 + P::OFF_P + tile_shift(C.e0, 24)) + 6 * s;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) pbc[f] = active ? spb[f] : 0;
+    }
+    const long base = static_cast<long>(e) * NP;
     // Every thread finished the previous tile (the barrier above), so its
     // slot is free: refill it with the tile NS iterations on from it.
     if (threadIdx.x == 0 && it > 0) {

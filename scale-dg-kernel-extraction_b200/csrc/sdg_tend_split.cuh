@@ -60,14 +60,16 @@ struct SplitPlan {
   static constexpr size_t EB = r16(sizeof(TC) * 3 + 32);
   static constexpr size_t FB = r16(sizeof(TC) * 6 + 32);
   static constexpr size_t PB = r16(sizeof(int) * 6 + 32);
+  static constexpr size_t CB = 128;  // a batched tile's TileCtx
   static constexpr size_t FACE = r16(sizeof(TC) * FaceArea<NQ, sizeof(TC) == 8>::ELEM);
   static constexpr size_t FLUX = r16(sizeof(TC) * 6 * NQ2);
   static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
   static constexpr size_t BARS = 16 * NSTAGE;
   static constexpr size_t REST = FACE + FLUX + LIFTB + BARS;
   static constexpr size_t SEP_BYTES =
-      NSTAGE * (QB + 3 * VB0 + EB + FB + PB) + 2 * LINE + REST;
-  static constexpr size_t ALIAS_BYTES = NSTAGE * (QB + 3 * mx(VB0, LINE) + EB + FB + PB) + REST;
+      NSTAGE * (QB + 3 * VB0 + EB + FB + PB + CB) + 2 * LINE + REST;
+  static constexpr size_t ALIAS_BYTES =
+      NSTAGE * (QB + 3 * mx(VB0, LINE) + EB + FB + PB + CB) + REST;
   static constexpr int blocks(size_t bytes) {
     return static_cast<int>(kSmemPerSM / (bytes + kSmemPerBlockReserved));
   }
@@ -86,7 +88,8 @@ struct SplitPlan {
   static constexpr size_t OFF_E = QB + 3 * VB;
   static constexpr size_t OFF_F = OFF_E + EB;
   static constexpr size_t OFF_P = OFF_F + FB;
-  static constexpr size_t SLOT = OFF_P + PB;
+  static constexpr size_t OFF_C = OFF_P + PB;
+  static constexpr size_t SLOT = OFF_C + CB;
   static constexpr size_t LINES = SEP ? 2 * LINE : 0;
   static constexpr size_t BYTES = NSTAGE * SLOT + LINES + REST;
   static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
@@ -180,6 +183,9 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     if (tile + 1 == A.inject_skip) return;
     const Ctx cx = tile_ctx<1, BATCH>(A, tile, ntiles);
     unsigned char* base = slots + slot * P::SLOT;
+    // A batched tile's context goes with it (read by the consumers from
+    // shared memory instead of the tile and instance tables).
+    if constexpr (BATCH) *reinterpret_cast<Ctx*>(base + P::OFF_C) = cx;
     const void* src[7] = {cx.q, cx.u, cx.v, cx.w, cx.escale, cx.fscale, cx.pbase};
     const size_t per[7] = {sizeof(TQ) * NP, sizeof(TV) * NP, sizeof(TV) * NP,
                            sizeof(TV) * NP, sizeof(TC) * 3,  sizeof(TC) * 6,
@@ -227,9 +233,8 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     if (tile >= ntiles) break;
     const int slot = it % NS;
     const uint32_t parity = (it / NS) & 1;
-    const Ctx C = tile_ctx<1, BATCH>(A, tile, ntiles);
-    const int e = C.e0;
-    const long base = static_cast<long>(e) * NP;
+    Ctx C;
+    if constexpr (!BATCH) C = tile_ctx<1, false>(A, tile, ntiles);
 
     // ---- Wait for the tile's slot (bounded, block-uniform) ---------------
     const bool ok = __syncthreads_and(mbar_wait_bounded(&bars[slot], parity, spins));
@@ -245,12 +250,15 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       }
       return;
     }
+    unsigned char* sb = slots + slot * P::SLOT;
+    if constexpr (BATCH) C = *reinterpret_cast<const Ctx*>(sb + P::OFF_C);
+    const int e = C.e0;
+    const long base = static_cast<long>(e) * NP;
     if (threadIdx.x == 0 && it > 0) {
       const int nt = blockIdx.x + (it - 1 + NS) * gridDim.x;
       if (nt < ntiles) issue(nt, (it - 1) % NS);
     }
 
-    unsigned char* sb = slots + slot * P::SLOT;
     const TQ* sq = reinterpret_cast<const TQ*>(sb + tile_shift(C.e0, sizeof(TQ) * NP));
     const uint32_t shv = tile_shift(C.e0, sizeof(TV) * NP);
     const TV* su = reinterpret_cast<const TV*>(sb + P::OFF_U + shv);
