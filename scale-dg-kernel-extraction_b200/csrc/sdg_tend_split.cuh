@@ -38,6 +38,13 @@ struct SplitGeo {
   static constexpr int KZ = (NQ + H - 1) / H;  // column nodes per thread
 };
 
+// Registers a thread keeps at least, which caps the resident blocks: 128 for
+// FP64 and 80 for FP32.  (FP64 at Nq = 10 with 80: three blocks of 224
+// threads per SM, 8 bytes of spill, measured 0.252 against 0.234 ms per RK
+// stage 2 with two blocks.)
+template <int NQ, typename TC>
+constexpr int kSplitRegFloor = sizeof(TC) == 8 ? 128 : 80;
+
 // Shared-memory plan: the ring of one-element slots (q, u, v, w and the
 // element's escale, fscale and face-neighbour rows), the x- and y-line
 // buffers, the minus-side face values (FaceArea), the face fluxes ((f1, f3)
@@ -45,7 +52,9 @@ struct SplitGeo {
 // lift's x/y factors, barriers.  The line buffers have space of their own
 // (SEP) where the plan fits, so phase 1 writes them directly; otherwise they
 // reuse the slot's u and v regions once every thread holds its column,
-// which costs a barrier.
+// which costs a barrier.  Where it gains a resident block the face fluxes
+// overwrite the minus-side values they were computed from (FLUX_ALIAS): each
+// thread writes only the face-area words it alone has read.
 template <int NQ, int H, typename TQ, typename TV, typename TC, bool STAGE>
 struct SplitPlan {
   static constexpr int NQ2 = NQ * NQ;
@@ -65,33 +74,46 @@ struct SplitPlan {
   static constexpr size_t FLUX = r16(sizeof(TC) * 6 * NQ2);
   static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
   static constexpr size_t BARS = 16 * NSTAGE;
-  static constexpr size_t REST = FACE + FLUX + LIFTB + BARS;
-  static constexpr size_t SEP_BYTES =
-      NSTAGE * (QB + 3 * VB0 + EB + FB + PB + CB) + 2 * LINE + REST;
-  static constexpr size_t ALIAS_BYTES =
-      NSTAGE * (QB + 3 * mx(VB0, LINE) + EB + FB + PB + CB) + REST;
-  static constexpr int blocks(size_t bytes) {
-    return static_cast<int>(kSmemPerSM / (bytes + kSmemPerBlockReserved));
+  // Bytes of the plan with separate line buffers (sep) and with the face
+  // fluxes in the face area (fal).  Without sep the u and v regions hold the
+  // line buffers; w holds q*w either way.
+  static constexpr size_t bytes_of(bool sep, bool fal) {
+    return NSTAGE * (QB + 2 * (sep ? VB0 : mx(VB0, LINE)) + VB0 + EB + FB + PB + CB) +
+           (sep ? 2 * LINE : 0) + FACE + (fal ? 0 : FLUX) + LIFTB + BARS;
   }
-  // Resident blocks the registers allow (at least 128 registers per FP64
-  // thread, 80 per FP32 thread; see split_min_blocks).
+  static constexpr size_t SEP_BYTES = bytes_of(true, false);
+  static constexpr size_t ALIAS_BYTES = bytes_of(false, false);
+  static constexpr int blocks(size_t bytes) {
+    return bytes > kPipeMaxSmem
+               ? 0
+               : static_cast<int>(kSmemPerSM / (bytes + kSmemPerBlockReserved));
+  }
+  // Resident blocks the registers allow (kSplitRegFloor registers a thread).
   static constexpr int REG_BLOCKS =
-      65536 / (((H * NQ2 + 31) / 32 * 32) * (sizeof(TC) == 8 ? 128 : 80));
+      65536 / (((H * NQ2 + 31) / 32 * 32) * kSplitRegFloor<NQ, TC>);
   static constexpr int cap(int b) { return b < REG_BLOCKS ? b : REG_BLOCKS; }
-  // Separate line buffers where they fit and cost no resident block.
-  static constexpr bool SEP =
-      SEP_BYTES <= kPipeMaxSmem && cap(blocks(SEP_BYTES)) >= cap(blocks(ALIAS_BYTES));
+  // The most resident blocks any layout reaches; the first layout that
+  // reaches it, in the order: separate line buffers, then separate fluxes.
+  static constexpr int BEST = mx(mx(cap(blocks(bytes_of(true, false))),
+                                    cap(blocks(bytes_of(true, true)))),
+                                 mx(cap(blocks(bytes_of(false, false))),
+                                    cap(blocks(bytes_of(false, true)))));
+  static constexpr bool SEP = cap(blocks(bytes_of(true, false))) == BEST ||
+                              cap(blocks(bytes_of(true, true))) == BEST;
+  static constexpr bool FLUX_ALIAS = cap(blocks(bytes_of(SEP, false))) < BEST;
   static constexpr size_t VB = SEP ? VB0 : mx(VB0, LINE);
   static constexpr size_t OFF_U = QB;
   static constexpr size_t OFF_V = QB + VB;
   static constexpr size_t OFF_W = QB + 2 * VB;
-  static constexpr size_t OFF_E = QB + 3 * VB;
+  static constexpr size_t OFF_E = OFF_W + VB0;
   static constexpr size_t OFF_F = OFF_E + EB;
   static constexpr size_t OFF_P = OFF_F + FB;
   static constexpr size_t OFF_C = OFF_P + PB;
   static constexpr size_t SLOT = OFF_C + CB;
   static constexpr size_t LINES = SEP ? 2 * LINE : 0;
+  static constexpr size_t REST = FACE + (FLUX_ALIAS ? 0 : FLUX) + LIFTB + BARS;
   static constexpr size_t BYTES = NSTAGE * SLOT + LINES + REST;
+  static_assert(BYTES == bytes_of(SEP, FLUX_ALIAS), "slot layout");
   static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
       kSmemPerSM / (BYTES + kSmemPerBlockReserved) > 4
           ? 4
@@ -100,26 +122,42 @@ struct SplitPlan {
                  : kSmemPerSM / (BYTES + kSmemPerBlockReserved)));
 };
 
+// A part of the column, as a type (the per-node phases are compiled once per
+// part; -1: the part known at run time only).
+template <int HH>
+struct Part {
+  static constexpr int value = HH;
+};
+
+// Orders whose per-node phases are compiled once per part, with node k a
+// compile-time constant, for the warps whose threads all hold the same part
+// (the one warp that straddles the two parts runs the run-time copy, so it
+// does not do both).  At Nq = 12 and 16 the copies make the register
+// allocator spill (0.8-4 KB a thread), so those keep the run-time copy.
+template <int NQ>
+constexpr bool kSplitPartCopies = NQ != 12 && NQ != 16;
+
 // Columns split in two from Nq = 9 on.
 template <int NQ>
 constexpr int kSplitH = 2;
 
 // Where the automatic variant takes the split-column kernel: the orders at
 // which it measured faster than tend_pipe_kernel (RK stage 2, ~16.8 M DOF,
-// ms split / pipelined): fast FP64 p = 8 0.266 / 0.271, p = 9 0.241 / 0.272,
-// p = 11 0.295 / 0.331, p = 12 0.310 / 0.344, p = 13 0.275 / 0.342; mixed
-// p = 11 0.144 / 0.151.  Slower at FP64 p = 10 and the other mixed orders.
+// ms split / pipelined): fast FP64 p = 8 0.266 / 0.271, p = 9 0.223 / 0.252,
+// p = 11 0.295 / 0.331, p = 12 0.295 / 0.316, p = 13 0.255 / 0.295; mixed
+// p = 11 0.144 / 0.151.  Slower at FP64 p = 10 and 14 (0.325 / 0.308) and
+// the other mixed orders.
 template <int NQ, typename TC, bool EXACT>
 constexpr bool kSplitAuto =
     !EXACT && (sizeof(TC) == 8 ? (NQ == 9 || NQ == 10 || (NQ >= 12 && NQ <= 14)) : NQ == 12);
 
 // Blocks per SM the kernel is built for: what the shared memory allows,
-// capped so that a thread keeps at least 128 (FP64) or 80 (FP32) registers.
+// capped so that a thread keeps at least kSplitRegFloor registers.
 template <int NQ, int H, typename TQ, typename TV, typename TC, bool STAGE>
 constexpr int split_min_blocks() {
   constexpr int m = SplitPlan<NQ, H, TQ, TV, TC, STAGE>::BLOCKS_PER_SM_SMEM;
   constexpr int thr = (SplitGeo<NQ, H>::THREADS + 31) / 32 * 32;
-  constexpr int floor_regs = sizeof(TC) == 8 ? 128 : 80;
+  constexpr int floor_regs = kSplitRegFloor<NQ, TC>;
   constexpr int by_regs = 65536 / (thr * floor_regs);
   constexpr int r = m < by_regs ? m : by_regs;
   return r < 1 ? 1 : r;
@@ -147,9 +185,10 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
   unsigned char* slots = smem_raw;
   unsigned char* rest = smem_raw + NS * P::SLOT + P::LINES;
   TC* fa = reinterpret_cast<TC*>(rest);
+  constexpr size_t FLUXB = P::FLUX_ALIAS ? 0 : P::FLUX;
   TC* flux = reinterpret_cast<TC*>(rest + P::FACE);
-  TC* sL = reinterpret_cast<TC*>(rest + P::FACE + P::FLUX);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(rest + P::FACE + P::FLUX + P::LIFTB);
+  TC* sL = reinterpret_cast<TC*>(rest + P::FACE + FLUXB);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(rest + P::FACE + FLUXB + P::LIFTB);
   constexpr bool SEP = P::SEP;
 
   const int h = threadIdx.x / NQ2;      // part of the column
@@ -161,6 +200,12 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
   const bool own_y = h == 0;            // y faces and the -z face
   const bool own_x = h == H - 1;        // x faces and the +z face
   const unsigned spins = A.wait_spins;
+  // The part of this warp's threads, or -1 when the warp holds both.
+  auto part_of_warp = [&]() {
+    const int t0 = threadIdx.x & ~31;
+    const int t1 = min(t0 + 31, static_cast<int>(blockDim.x) - 1);
+    return (t0 / NQ2 == t1 / NQ2) ? t0 / NQ2 : -1;
+  };
 
   // Minus-side face values (FaceArea): FP64 keeps the x faces in two scalar
   // arrays and the y faces as (q, v) pairs; FP32 keeps (q, un) pairs of the
@@ -172,10 +217,18 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
   V2* ypair = reinterpret_cast<V2*>(fa + FA::Y0);
   V2* fM = reinterpret_cast<V2*>(fa);
   // Face fluxes: (f1, f3) and (f2, f4) at face node n, f5 and f6 at column n.
-  V2* fl13 = reinterpret_cast<V2*>(flux);
-  V2* fl24 = fl13 + NQ2;
-  TC* fl5 = flux + 4 * NQ2;
-  TC* fl6 = flux + 5 * NQ2;
+  // With FLUX_ALIAS, in the face area: (f1, f3) over the -y pair of face
+  // node n, f5 over the +y pair's first word; FP64: f2, f4 and f6 over the
+  // x arrays' words xq[n], xq[XOFF + n] and xu[n]; FP32: (f2, f4) over the
+  // +x pair, f6 over the -x pair's first word.
+  constexpr bool FAL = P::FLUX_ALIAS;
+  V2* fl13 = FAL ? (XSPLIT ? ypair : fM) : reinterpret_cast<V2*>(flux);
+  V2* fl24 = FAL ? fM + NQ2 : reinterpret_cast<V2*>(flux) + NQ2;
+  TC* fl5 = FAL ? reinterpret_cast<TC*>(XSPLIT ? ypair + NQ2 : fM + 2 * NQ2) : flux + 4 * NQ2;
+  TC* fl6 = FAL ? (XSPLIT ? xu : reinterpret_cast<TC*>(fM + 3 * NQ2)) : flux + 5 * NQ2;
+  // Word stride of f5 and f6 between columns (pairs in the aliased form).
+  constexpr int S5 = FAL ? 2 : 1;
+  constexpr int S6 = (FAL && !XSPLIT) ? 2 : 1;
 
   // Producer: one thread fills ring slot `slot` with tile (element) `tile`.
   auto issue = [&](int tile, int slot) {
@@ -315,9 +368,16 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     if constexpr (SEP) load_q0();
 
     // ---- Phase 1: this thread's nodes of column c -------------------------
+    // The per-node phases run in a copy per part h (kSplitPartCopies), so
+    // that node k is a compile-time constant: the coefficients D(k, l) and
+    // the z-lift factors are then immediate constant-bank operands, not
+    // indexed constant loads.
+    constexpr bool PC = kSplitPartCopies<NQ>;
+    const int hw = PC ? part_of_warp() : -1;  // the warp's part, -1: mixed
     TC fx[KZ], fy[KZ];
     TC wlo = TC(0), whi = TC(0), qlo = TC(0), qhi = TC(0);
-    {
+    auto phase1 = [&](auto part) __attribute__((always_inline)) {
+      const int K0 = decltype(part)::value >= 0 ? decltype(part)::value * KZ : k0;
       const bool onx = (a == 0) || (a == NQ - 1);
       const bool ony = (b == 0) || (b == NQ - 1);
       const int xo = (a == 0 ? FA::XOFF : 0) + b;
@@ -325,7 +385,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       V2* fmy = XSPLIT ? ypair + (b == 0 ? 0 : NQ2) + a : fM + (b == 0 ? 0 : 2) * NQ2 + a;
 #pragma unroll
       for (int kk = 0; kk < KZ; ++kk) {
-        const int k = k0 + kk;
+        const int k = K0 + kk;
         if (KZ * H != NQ && k >= NQ) break;
         const int n = c + NQ2 * k;
         const TC qv = static_cast<TC>(sq[n]);
@@ -357,7 +417,13 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         }
         if (ony) fmy[NQ * k] = V2{qv, vv};
       }
-    }
+    };
+    if (hw < 0)
+      phase1(Part<-1>{});
+    else if (hw == 0)
+      phase1(Part<0>{});
+    else
+      phase1(Part<1>{});
     // The slot's writes (q*w; line buffers in u, v without SEP) come before
     // the refill that overwrites it.
     fence_proxy_async_smem();
@@ -416,7 +482,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       const TC f1 = upwind_flux<AR, TC>(m1.x, m1.y, qP[0], unP[0], TC(-1), sfs[0]);
       const TC f3 = upwind_flux<AR, TC>(m3.x, m3.y, qP[1], unP[1], TC(1), sfs[2]);
       fl13[c] = V2{f1, f3};
-      fl5[c] = upwind_flux<AR, TC>(qlo, wlo, qP[2], unP[2], TC(-1), sfs[4]);
+      fl5[S5 * c] = upwind_flux<AR, TC>(qlo, wlo, qP[2], unP[2], TC(-1), sfs[4]);
     }
     if (own_x) {
       // x faces at face node c: +x (2) and -x (4); +z (6) of column c.
@@ -436,13 +502,19 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       }
       const TC f2 = upwind_flux<AR, TC>(q2, u2, qP[0], unP[0], TC(1), sfs[1]);
       const TC f4 = upwind_flux<AR, TC>(q4, u4, qP[1], unP[1], TC(-1), sfs[3]);
-      fl24[c] = V2{f2, f4};
-      fl6[c] = upwind_flux<AR, TC>(qhi, whi, qP[2], unP[2], TC(1), sfs[5]);
+      if constexpr (FAL && XSPLIT) {
+        xq[c] = f2;
+        xq[FA::XOFF + c] = f4;
+      } else {
+        fl24[c] = V2{f2, f4};
+      }
+      fl6[S6 * c] = upwind_flux<AR, TC>(qhi, whi, qP[2], unP[2], TC(1), sfs[5]);
     }
     __syncthreads();
 
     // ---- Epilogue: z-derivative, lift, combine, store ---------------------
-    {
+    auto epilogue = [&](auto part) __attribute__((always_inline)) {
+      const int K0 = decltype(part)::value >= 0 ? decltype(part)::value * KZ : k0;
       const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
       TC lxy[4];
       if constexpr (!EXACT) {
@@ -451,13 +523,13 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         lxy[2] = sL[2 * NQ + b];
         lxy[3] = sL[3 * NQ + a];
       }
-      const TC f5 = fl5[c], f6 = fl6[c];
+      const TC f5 = fl5[S5 * c], f6 = fl6[S6 * c];
       TC fz[NQ];
 #pragma unroll
       for (int l = 0; l < NQ; ++l) fz[l] = sz[c + NQ2 * l];
 #pragma unroll
       for (int kk = 0; kk < KZ; ++kk) {
-        const int k = k0 + kk;
+        const int k = K0 + kk;
         if (KZ * H != NQ && k >= NQ) break;
         const TC dz = contract<NQ, ORDER, AR, TC>([&](int l) { return fz[l]; },
                                                   [&](int l) { return D.d[k * NQ + l]; });
@@ -473,7 +545,13 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         }
         // tensorprod_Lift_hexahedral (kern:278-283), face order 1..6.
         const V2 f13 = fl13[a + NQ * k];
-        const V2 f24 = fl24[b + NQ * k];
+        V2 f24;
+        if constexpr (FAL && XSPLIT) {
+          f24.x = xq[b + NQ * k];
+          f24.y = xq[FA::XOFF + b + NQ * k];
+        } else {
+          f24 = fl24[b + NQ * k];
+        }
         TC lf = AR::mul(L[0], f13.x);
         lf = AR::mad(L[1], f24.x, lf);
         lf = AR::mad(L[2], f13.y, lf);
@@ -498,7 +576,13 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
           C.out[n] = static_cast<TO>(r);
         }
       }
-    }
+    };
+    if (hw < 0)
+      epilogue(Part<-1>{});
+    else if (hw == 0)
+      epilogue(Part<0>{});
+    else
+      epilogue(Part<1>{});
   }
 }
 
