@@ -105,7 +105,8 @@ int run(const LaunchSpec& s) {
                            (EXACT || s.lift_z != nullptr) &&
                            (batch || (aligned(s.q) && aligned(s.u) && aligned(s.v) &&
                                       aligned(s.w) && aligned(s.escale) &&
-                                      aligned(s.fscale) && aligned(s.pbase)));
+                                      aligned(s.fscale) && aligned(s.pbase) &&
+                                      (s.q0 == nullptr || aligned(s.q0))));
     const bool want_split =
         s.variant == kVariantSplit ||
         (s.variant == kVariantAuto && !batch && kSplitAuto<NQ, TC, EXACT>);

@@ -45,16 +45,27 @@ struct SplitGeo {
 template <int NQ, typename TC>
 constexpr int kSplitRegFloor = sizeof(TC) == 8 ? 128 : 80;
 
+// Where the RK base state q0 may travel in the ring slot (a bulk copy with
+// the tile's other inputs, read from shared memory by the epilogue) rather
+// than be loaded into registers from L2: it frees KZ registers for the
+// whole tile.  Measured (RK stage 2, ~16.8 M DOF, ms in the slot / from L2):
+// FP64 p = 8 0.255 / 0.264, p = 11 0.290 / 0.296, p = 12 0.274 / 0.294;
+// mixed p = 9 0.143 / 0.151; slower at FP64 p = 9 (0.230 / 0.226).  The plan
+// takes it where it costs no resident block and no separate line buffers.
+template <int NQ, typename TC>
+constexpr bool kSplitRingQ0 = !(sizeof(TC) == 8 && NQ == 10);
+
 // Shared-memory plan: the ring of one-element slots (q, u, v, w and the
 // element's escale, fscale and face-neighbour rows), the x- and y-line
 // buffers, the minus-side face values (FaceArea), the face fluxes ((f1, f3)
 // and (f2, f4) pairs per face node, f5 and f6 per column), the factored
-// lift's x/y factors, barriers.  The line buffers have space of their own
-// (SEP) where the plan fits, so phase 1 writes them directly; otherwise they
-// reuse the slot's u and v regions once every thread holds its column,
-// which costs a barrier.  Where it gains a resident block the face fluxes
-// overwrite the minus-side values they were computed from (FLUX_ALIAS): each
-// thread writes only the face-area words it alone has read.
+// lift's x/y factors, barriers; q0 in the slot where RING_Q0.  The line
+// buffers have space of their own (SEP) where the plan fits, so phase 1
+// writes them directly; otherwise they reuse the slot's u and v regions once
+// every thread holds its column, which costs a barrier.  Where it gains a
+// resident block the face fluxes overwrite the minus-side values they were
+// computed from (FLUX_ALIAS): each thread writes only the face-area words it
+// alone has read.
 template <int NQ, int H, typename TQ, typename TV, typename TC, bool STAGE>
 struct SplitPlan {
   static constexpr int NQ2 = NQ * NQ;
@@ -74,15 +85,19 @@ struct SplitPlan {
   static constexpr size_t FLUX = r16(sizeof(TC) * 6 * NQ2);
   static constexpr size_t LIFTB = r16(sizeof(TC) * 4 * NQ);
   static constexpr size_t BARS = 16 * NSTAGE;
-  // Bytes of the plan with separate line buffers (sep) and with the face
-  // fluxes in the face area (fal).  Without sep the u and v regions hold the
-  // line buffers; w holds q*w either way.
-  static constexpr size_t bytes_of(bool sep, bool fal) {
-    return NSTAGE * (QB + 2 * (sep ? VB0 : mx(VB0, LINE)) + VB0 + EB + FB + PB + CB) +
+  // The RK base state q0 of the tile (stages 2-3), when it travels in the
+  // slot.
+  static constexpr size_t Q0B = STAGE ? r16(sizeof(double) * NP + 32) : 0;
+  // Bytes of the plan with separate line buffers (sep), with the face
+  // fluxes in the face area (fal) and with q0 in the slot (rq).  Without sep
+  // the u and v regions hold the line buffers; w holds q*w either way.
+  static constexpr size_t bytes_of(bool sep, bool fal, bool rq) {
+    return NSTAGE * (QB + 2 * (sep ? VB0 : mx(VB0, LINE)) + VB0 + EB + FB + PB + CB +
+                     (rq ? Q0B : 0)) +
            (sep ? 2 * LINE : 0) + FACE + (fal ? 0 : FLUX) + LIFTB + BARS;
   }
-  static constexpr size_t SEP_BYTES = bytes_of(true, false);
-  static constexpr size_t ALIAS_BYTES = bytes_of(false, false);
+  static constexpr size_t SEP_BYTES = bytes_of(true, false, false);
+  static constexpr size_t ALIAS_BYTES = bytes_of(false, false, false);
   static constexpr int blocks(size_t bytes) {
     return bytes > kPipeMaxSmem
                ? 0
@@ -92,15 +107,30 @@ struct SplitPlan {
   static constexpr int REG_BLOCKS =
       65536 / (((H * NQ2 + 31) / 32 * 32) * kSplitRegFloor<NQ, TC>);
   static constexpr int cap(int b) { return b < REG_BLOCKS ? b : REG_BLOCKS; }
-  // The most resident blocks any layout reaches; the first layout that
-  // reaches it, in the order: separate line buffers, then separate fluxes.
-  static constexpr int BEST = mx(mx(cap(blocks(bytes_of(true, false))),
-                                    cap(blocks(bytes_of(true, true)))),
-                                 mx(cap(blocks(bytes_of(false, false))),
-                                    cap(blocks(bytes_of(false, true)))));
-  static constexpr bool SEP = cap(blocks(bytes_of(true, false))) == BEST ||
-                              cap(blocks(bytes_of(true, true))) == BEST;
-  static constexpr bool FLUX_ALIAS = cap(blocks(bytes_of(SEP, false))) < BEST;
+  // The most resident blocks any layout reaches, and the first layout that
+  // reaches it in the order of preference: separate line buffers, then q0
+  // in the slot, then separate fluxes.  Layout index L: bit 2 sep, bit 1 rq,
+  // bit 0 !fal.
+  static constexpr int blocks_of(int L) {
+    return cap(blocks(bytes_of((L & 4) != 0, (L & 1) == 0, (L & 2) != 0)));
+  }
+  static constexpr int best_blocks() {
+    int b = 0;
+    for (int L = 0; L < 8; ++L) b = blocks_of(L) > b ? blocks_of(L) : b;
+    return b;
+  }
+  static constexpr int BEST = best_blocks();
+  static constexpr int pick() {
+    for (int L = 7; L >= 0; --L) {
+      if (!kSplitRingQ0<NQ, TC> && (L & 2)) continue;
+      if (blocks_of(L) == BEST) return L;
+    }
+    return 0;
+  }
+  static constexpr int LAYOUT = pick();
+  static constexpr bool SEP = (LAYOUT & 4) != 0;
+  static constexpr bool RING_Q0 = STAGE && (LAYOUT & 2) != 0;
+  static constexpr bool FLUX_ALIAS = (LAYOUT & 1) == 0;
   static constexpr size_t VB = SEP ? VB0 : mx(VB0, LINE);
   static constexpr size_t OFF_U = QB;
   static constexpr size_t OFF_V = QB + VB;
@@ -109,11 +139,12 @@ struct SplitPlan {
   static constexpr size_t OFF_F = OFF_E + EB;
   static constexpr size_t OFF_P = OFF_F + FB;
   static constexpr size_t OFF_C = OFF_P + PB;
-  static constexpr size_t SLOT = OFF_C + CB;
+  static constexpr size_t OFF_Q0 = OFF_C + CB;
+  static constexpr size_t SLOT = OFF_Q0 + (RING_Q0 ? Q0B : 0);
   static constexpr size_t LINES = SEP ? 2 * LINE : 0;
   static constexpr size_t REST = FACE + (FLUX_ALIAS ? 0 : FLUX) + LIFTB + BARS;
   static constexpr size_t BYTES = NSTAGE * SLOT + LINES + REST;
-  static_assert(BYTES == bytes_of(SEP, FLUX_ALIAS), "slot layout");
+  static_assert(BYTES == bytes_of(SEP, FLUX_ALIAS, RING_Q0), "slot layout");
   static constexpr int BLOCKS_PER_SM_SMEM = static_cast<int>(
       kSmemPerSM / (BYTES + kSmemPerBlockReserved) > 4
           ? 4
@@ -143,13 +174,14 @@ constexpr int kSplitH = 2;
 
 // Where the automatic variant takes the split-column kernel: the orders at
 // which it measured faster than tend_pipe_kernel (RK stage 2, ~16.8 M DOF,
-// ms split / pipelined): fast FP64 p = 8 0.266 / 0.271, p = 9 0.223 / 0.252,
-// p = 11 0.295 / 0.331, p = 12 0.295 / 0.316, p = 13 0.255 / 0.295; mixed
-// p = 11 0.144 / 0.151.  Slower at FP64 p = 10 and 14 (0.325 / 0.308) and
-// the other mixed orders.
+// ms split / pipelined): fast FP64 p = 8 0.255 / 0.263, p = 9 0.226 / 0.254,
+// p = 11 0.290 / 0.327, p = 12 0.274 / 0.319, p = 13 0.256 / 0.299; mixed
+// p = 9 0.143 / 0.159, p = 11 0.142 / 0.148.  Slower at FP64 p = 10 and 14
+// (0.244 / 0.233, 0.332 / 0.313) and the other mixed orders.
 template <int NQ, typename TC, bool EXACT>
 constexpr bool kSplitAuto =
-    !EXACT && (sizeof(TC) == 8 ? (NQ == 9 || NQ == 10 || (NQ >= 12 && NQ <= 14)) : NQ == 12);
+    !EXACT && (sizeof(TC) == 8 ? (NQ == 9 || NQ == 10 || (NQ >= 12 && NQ <= 14))
+                               : (NQ == 10 || NQ == 12));
 
 // Blocks per SM the kernel is built for: what the shared memory allows,
 // capped so that a thread keeps at least kSplitRegFloor registers.
@@ -251,16 +283,26 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       tile_range(cx.e0, cx.n, per[k], &lo[k], &by[k], &sh[k]);
       total += by[k];
     }
+    // q0 (RK stages 2-3): into the slot where the plan holds it, else
+    // into L2 for the epilogue's loads.
+    size_t l0 = 0;
+    uint32_t b0 = 0, s0 = 0;
+    const bool q0_used = STAGE && A.rk_a != 0.0;
+    if (q0_used) {
+      tile_range(cx.e0, cx.n, sizeof(double) * NP, &l0, &b0, &s0);
+      if constexpr (P::RING_Q0) total += b0;
+    }
     mbar_arrive_expect_tx(&bars[slot], total);
 #pragma unroll
     for (int k = 0; k < 7; ++k)
       bulk_g2s(base + off[k], static_cast<const unsigned char*>(src[k]) + lo[k], by[k],
                &bars[slot]);
-    if (STAGE && A.rk_a != 0.0) {
-      size_t l0;
-      uint32_t b0, s0;
-      tile_range(cx.e0, cx.n, sizeof(double) * NP, &l0, &b0, &s0);
-      bulk_prefetch_l2(reinterpret_cast<const unsigned char*>(cx.q0) + l0, b0);
+    if (q0_used) {
+      const unsigned char* q0src = reinterpret_cast<const unsigned char*>(cx.q0) + l0;
+      if constexpr (P::RING_Q0)
+        bulk_g2s(base + P::OFF_Q0, q0src, b0, &bars[slot]);
+      else
+        bulk_prefetch_l2(q0src, b0);
     }
   };
 
@@ -320,6 +362,8 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     const TC* ses = reinterpret_cast<const TC*>(sb + P::OFF_E + tile_shift(C.e0, sizeof(TC) * 3));
     const TC* sfs = reinterpret_cast<const TC*>(sb + P::OFF_F + tile_shift(C.e0, sizeof(TC) * 6));
     const int* spb = reinterpret_cast<const int*>(sb + P::OFF_P + tile_shift(C.e0, 24));
+    const double* sq0 = reinterpret_cast<const double*>(
+        sb + P::OFF_Q0 + tile_shift(C.e0, sizeof(double) * NP));
     static_assert(sizeof(TV) == sizeof(TC), "w and q*w share their slots");
     TC* sz = reinterpret_cast<TC*>(sb + P::OFF_W + shv);
     TC* sX = SEP ? reinterpret_cast<TC*>(smem_raw + NS * P::SLOT)
@@ -354,7 +398,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     double q0r[STAGE ? KZ : 1];
     const bool use_q0 = STAGE && A.rk_a != 0.0;
     auto load_q0 = [&]() {
-      if constexpr (STAGE) {
+      if constexpr (STAGE && !P::RING_Q0) {
         if (use_q0) {
 #pragma unroll
           for (int kk = 0; kk < KZ; ++kk) {
@@ -572,7 +616,12 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
           using AD = Ar<double, EXACT>;
           const double qd = static_cast<double>(sq[c + NQ2 * k]);
           double r = AD::mul(A.rk_b, AD::mad(C.dt, static_cast<double>(dqdt), qd));
-          if (use_q0) r = AD::mad(A.rk_a, q0r[kk], r);
+          if (use_q0) {
+            if constexpr (P::RING_Q0)
+              r = AD::mad(A.rk_a, sq0[c + NQ2 * k], r);
+            else
+              r = AD::mad(A.rk_a, q0r[kk], r);
+          }
           C.out[n] = static_cast<TO>(r);
         }
       }
