@@ -10,8 +10,11 @@ Metric: DOF-updates per second per RHS evaluation = Ne*Np*3*K / time.
   value  device-resident state, K steps timed with CUDA events on the
          library's stream (inputs of 537 MB > 126 MB L2, so no L2 flush).
   e2e    the same steps through the C ABI with host buffers: each step
-         uploads the state q from pinned host memory (sdg_set_field), runs
-         the step (sdg_rk3_steps) and reads q back (sdg_get_field).
+         uploads the state q from pinned host memory, runs the step and
+         reads q back into that memory, in one call (sdg_rk3_steps_host,
+         which overlaps the copies with the stages chunk by chunk); the
+         next step starts from the host copy.  e2e.three_calls: the same
+         with sdg_set_field + sdg_rk3_steps + sdg_get_field per step.
   e2e_cal_tend  the drop-in advect3d_eq_cal_tend call (sdg_cal_tend):
          q,u,v,w(Np,NeA) in, dqdt(Np,Ne) out per RHS evaluation.
   roofline  the fused stage kernel: algorithmic bytes (40/48/48 B per DOF
@@ -639,15 +642,24 @@ def run_ours(args):
     NE = mesh.Np * mesh.Ne
     q_pin = torch.empty(NE, dtype=torch.float64, pin_memory=True)
     q_pin.numpy()[:] = q.reshape(-1, order="F")[:NE]
+    qp = q_pin.numpy()
+    H.rk3_steps_host(qp, dt, 1)  # first-use set-up (chunk tables, streams)
+    qp[:] = q.reshape(-1, order="F")[:NE]
     rep.barrier()
     t0 = time.perf_counter()
-    qp = q_pin.numpy()
+    for _ in range(n_e2e):
+        H.rk3_steps_host(qp, dt, 1)
+    t_e2e = rep.max(time.perf_counter() - t0)
+    e2e = world * dof * 3 * n_e2e / t_e2e
+    qp[:] = q.reshape(-1, order="F")[:NE]
+    rep.barrier()
+    t0 = time.perf_counter()
     for _ in range(n_e2e):
         H.set_field(sdg.FIELD_Q, qp)
         H.rk3_steps(dt, 1)
         H.get_field(sdg.FIELD_Q, out=qp)
-    t_e2e = rep.max(time.perf_counter() - t0)
-    e2e = world * dof * 3 * n_e2e / t_e2e
+    t_e2e3 = rep.max(time.perf_counter() - t0)
+    e2e3 = world * dof * 3 * n_e2e / t_e2e3
 
     # ---- e2e of the drop-in tendency call (FP64 handles only) ----
     e2e_ct = None
@@ -714,7 +726,9 @@ def run_ours(args):
             "roofline": head["roofline"],
             "e2e": {"value": e2e, "unit": METRIC,
                     "h2d_bytes_per_step": NE * 8, "d2h_bytes_per_step": NE * 8,
-                    "api": "sdg_set_field + sdg_rk3_steps + sdg_get_field per step"},
+                    "api": "sdg_rk3_steps_host per step (pinned q in and out)",
+                    "three_calls": {"value": e2e3, "unit": METRIC,
+                                    "api": "sdg_set_field + sdg_rk3_steps + sdg_get_field"}},
             "e2e_cal_tend": e2e_ct,
             "accuracy": accuracy,
             "cpu_baseline": cpu,

@@ -424,8 +424,8 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       const int K0 = decltype(part)::value >= 0 ? decltype(part)::value * KZ : k0;
       const bool onx = (a == 0) || (a == NQ - 1);
       const bool ony = (b == 0) || (b == NQ - 1);
-      const int xo = (a == 0 ? FA::XOFF : 0) + b;
-      V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
+      [[maybe_unused]] const int xo = (a == 0 ? FA::XOFF : 0) + b;
+      [[maybe_unused]] V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
       V2* fmy = XSPLIT ? ypair + (b == 0 ? 0 : NQ2) + a : fM + (b == 0 ? 0 : 2) * NQ2 + a;
 #pragma unroll
       for (int kk = 0; kk < KZ; ++kk) {
@@ -560,7 +560,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     auto epilogue = [&](auto part) __attribute__((always_inline)) {
       const int K0 = decltype(part)::value >= 0 ? decltype(part)::value * KZ : k0;
       const TC e1 = ses[0], e2 = ses[1], e3 = ses[2];
-      TC lxy[4];
+      [[maybe_unused]] TC lxy[4];
       if constexpr (!EXACT) {
         lxy[0] = sL[b];
         lxy[1] = sL[NQ + a];

@@ -81,6 +81,16 @@ module mod_dg_gpu
       real(c_double), value :: dt
       integer(c_int), value :: nsteps
     end function
+    !> sdg_set_field(q) + sdg_rk3_steps + sdg_get_field(q) in one call, with
+    !! the copies overlapping the stages chunk by chunk (q pinned for that).
+    integer(c_int) function sdg_rk3_steps_host(h, q, dt, nsteps) &
+        bind(C, name="sdg_rk3_steps_host")
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: h
+      real(c_double), intent(inout) :: q(*)
+      real(c_double), value :: dt
+      integer(c_int), value :: nsteps
+    end function
     integer(c_int) function sdg_minmax(h, qmin, qmax) bind(C, name="sdg_minmax")
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: h

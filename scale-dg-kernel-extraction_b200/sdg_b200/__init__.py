@@ -72,6 +72,7 @@ SIGNATURES = {
     "sdg_set_field": (_I, [_P, _I, _P]),
     "sdg_get_field": (_I, [_P, _I, _P]),
     "sdg_rk3_steps": (_I, [_P, _D, _I]),
+    "sdg_rk3_steps_host": (_I, [_P, _P, _D, _I]),
     "sdg_minmax": (_I, [_P, _P, _P]),
     "sdg_diagnostics": (_I, [_P, _P, _D, _P, _P]),
     "sdg_synchronize": (_I, [_P]),
@@ -330,6 +331,20 @@ class Handle:
 
     def rk3_steps(self, dt, nsteps):
         _check(lib().sdg_rk3_steps(self._h, dt, nsteps))
+
+    def rk3_steps_host(self, q, dt, nsteps):
+        """set_field(q) + rk3_steps(dt, nsteps) + get_field(out=q) in one
+        pipelined call (sdg_rk3_steps_host): q, a contiguous float64 array
+        of at least Np*Ne values (pinned for the copies to overlap), is
+        updated in place."""
+        if not (isinstance(q, np.ndarray) and q.dtype == np.float64 and
+                (q.flags.c_contiguous or q.flags.f_contiguous) and q.flags.writeable):
+            raise SdgError(SDG_ERR_ARG, "rk3_steps_host: q must be a writable contiguous "
+                           "float64 array")
+        if q.size < self.mesh.Np * self.mesh.Ne:
+            raise SdgError(SDG_ERR_ARG, "field smaller than (Np, Ne)")
+        _check(lib().sdg_rk3_steps_host(self._h, _p(q), dt, nsteps))
+        return q
 
     def rk3_stage(self, stage, dt):
         """One stage (1..3) of an RK3 step, without a graph."""

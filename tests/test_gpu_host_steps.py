@@ -1,0 +1,109 @@
+"""sdg_rk3_steps_host: the pipelined host-buffer RK call equals
+sdg_set_field + sdg_rk3_steps + sdg_get_field bit for bit (needs a B200).
+
+The call cuts the element range into chunks (runs of z-layers in a box)
+and runs the first and last steps chunk by chunk while the state's chunks
+go up and come back; every element still sees exactly the kernels of the
+resident path, so the state matches to the last bit.  Cases: chunk
+boundaries on and off the z-layers, FP64 fast and exact, the mixed form,
+one to three steps, the unchunked path of a small mesh, and the handle
+still usable afterwards.
+"""
+import numpy as np
+import pytest
+import torch
+
+import sdg_b200 as sdg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build(built):
+    return built
+
+
+def make(dims, p, flags, seed=3):
+    ops = sdg.read_operators(p)
+    mesh = sdg.mesh_setup(*dims, p, ops.x1D)
+    q, u, v, w = sdg.init_fields(mesh, ic_kind=1, seed=seed, vel_kind=1,
+                                 vel=(1.0, 0.5, 0.25))
+    dt = 0.1 / max(dims) / (p + 1) ** 2
+    return ops, mesh, (q, u, v, w), dt
+
+
+def three_calls(ops, mesh, flags, fields, dt, nsteps):
+    h = sdg.Handle(ops, mesh, flags)
+    h.set_state(*fields)
+    h.rk3_steps(dt, nsteps)
+    out = h.get_field()
+    h.close()
+    return out
+
+
+def pinned_copy(q, mesh):
+    n = mesh.Np * mesh.Ne
+    t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    a = t.numpy()
+    a[:] = np.asarray(q).reshape(-1, order="F")[:n]
+    return t, a
+
+
+@pytest.mark.parametrize("dims,p,flags,nsteps", [
+    ((16, 16, 16), 3, 0, 1),                    # 8 chunks of two z-layers
+    ((13, 16, 20), 2, 0, 2),                    # chunk edges inside z-layers
+    ((16, 16, 8), 1, sdg.FLAG_EXACT, 3),        # 4 chunks, exact arithmetic
+    ((16, 16, 16), 3, sdg.FLAG_MIXED, 2),       # mixed form
+    ((12, 12, 16), 7, 0, 1),                    # DMMA lines, two elements a tile
+    ((8, 8, 32), 9, 0, 1),                      # split-column kernel
+    ((4, 4, 4), 3, 0, 2),                       # too small: the three calls
+])
+def test_host_steps_equal_three_calls(dims, p, flags, nsteps):
+    ops, mesh, fields, dt = make(dims, p, flags)
+    ref = three_calls(ops, mesh, flags, fields, dt, nsteps)
+    h = sdg.Handle(ops, mesh, flags)
+    for which, a in zip((sdg.FIELD_U, sdg.FIELD_V, sdg.FIELD_W), fields[1:]):
+        h.set_field(which, a)
+    _keep, qp = pinned_copy(fields[0], mesh)
+    h.rk3_steps_host(qp, dt, nsteps)
+    got = qp.reshape(mesh.Np, mesh.Ne, order="F")
+    assert np.array_equal(got, ref)
+    # The handle's resident state is the same state: two more steps on the
+    # device agree with two more through the three calls.
+    h.rk3_steps(dt, 2)
+    more = h.get_field()
+    h.close()
+    ref2 = three_calls(ops, mesh, flags, (ref,) + tuple(fields[1:]), dt, 2)
+    assert np.array_equal(more, ref2)
+
+
+def test_host_steps_repeat_and_pageable_memory():
+    """Repeated calls chain like repeated three-call steps; pageable host
+    memory gives the same result (the copies just do not overlap)."""
+    ops, mesh, fields, dt = make((16, 16, 16), 2, 0)
+    ref = three_calls(ops, mesh, 0, fields, dt, 3)
+    h = sdg.Handle(ops, mesh, 0)
+    for which, a in zip((sdg.FIELD_U, sdg.FIELD_V, sdg.FIELD_W), fields[1:]):
+        h.set_field(which, a)
+    q = np.array(fields[0][:, : mesh.Ne], order="F")
+    for _ in range(3):
+        h.rk3_steps_host(q, dt, 1)
+    h.close()
+    assert np.array_equal(q, ref)
+
+
+def test_host_steps_argument_errors():
+    ops, mesh, fields, dt = make((16, 16, 8), 1, 0)
+    h = sdg.Handle(ops, mesh, 0)
+    q = np.array(fields[0][:, : mesh.Ne], order="F")
+    with pytest.raises(sdg.SdgError):
+        h.rk3_steps_host(q, dt, 1)          # velocities not set
+    for which, a in zip((sdg.FIELD_U, sdg.FIELD_V, sdg.FIELD_W), fields[1:]):
+        h.set_field(which, a)
+    with pytest.raises(sdg.SdgError):
+        h.rk3_steps_host(q, dt, -1)
+    with pytest.raises(sdg.SdgError):
+        h.rk3_steps_host(q[:, :3].copy(order="F"), dt, 1)   # too small
+    h.rk3_steps_host(q, dt, 0)              # upload and download only
+    assert np.array_equal(q, fields[0][:, : mesh.Ne])
+    h.close()
