@@ -235,12 +235,17 @@ struct sdg_handle {
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0.0;
 
-  // sdg_rk3_steps_host (lazy): element chunks (boundaries, S + 1 of them;
-  // empty when the mesh does not pipeline), each chunk's face-neighbour
-  // chunks (itself included), the copy streams and per-chunk events.
+  // sdg_rk3_steps_host and sdg_cal_tend (lazy): element chunks (boundaries,
+  // S + 1 of them; empty when the mesh is too small to pipeline), each
+  // chunk's face-neighbour chunks (itself included) through the direct
+  // table (empty when a face reads the halo) and through the halo table
+  // (with chunk_halo[j]: a face of chunk j reads the halo buffer), the copy
+  // streams and per-chunk events.
   bool chunks_built = false;
   std::vector<int> chunk_e0;
   std::vector<std::vector<int>> chunk_nbr;
+  std::vector<std::vector<int>> chunk_nbr_h;
+  std::vector<char> chunk_halo;
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   std::vector<cudaEvent_t> ev_up, ev_fin;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -556,10 +561,13 @@ int ensure_graph(sdg_handle* h, double dt) {
   return SDG_OK;
 }
 
-// Element chunks of sdg_rk3_steps_host: S contiguous element ranges (at most
-// 16, at least 512 elements each; fewer than 4 chunks, or a mesh whose
-// boundary faces read the halo buffer, do not pipeline) and, per chunk, the
-// chunks that hold a face neighbour of one of its elements.  Elements are
+// Element chunks of sdg_rk3_steps_host and sdg_cal_tend: S contiguous
+// element ranges (at most 16, at least 512 elements each; fewer than 4
+// chunks do not pipeline) and, per chunk, the chunks that hold a face
+// neighbour of one of its elements, through the direct table (the RK path;
+// it does not pipeline when a boundary face reads the halo buffer) and
+// through the halo table (the tendency call, which reads the caller's
+// halo).  Elements are
 // numbered x fastest, so in a box each chunk is a run of z-layers and its
 // neighbours are the chunks before and after it (cyclically).  The chunk
 // count trades the tail (the last upload's neighbours, about six chunks,
@@ -570,33 +578,49 @@ int build_chunks(sdg_handle* h) {
   if (h->chunks_built) return SDG_OK;
   h->chunks_built = true;
   const int S = std::min(16, h->Ne / 512);
-  if (!h->direct_ok || S < 4) return SDG_OK;
-  std::vector<int> pb(6 * static_cast<size_t>(h->Ne));
-  SDG_CUDA(cudaMemcpy(pb.data(), h->pb_direct, pb.size() * sizeof(int),
-                      cudaMemcpyDeviceToHost));
+  if (S < 4) return SDG_OK;
   std::vector<int> e0(S + 1);
   for (int j = 0; j <= S; ++j) e0[j] = static_cast<int>(static_cast<long>(h->Ne) * j / S);
+  auto chunk_of = [&](int e) {
+    return static_cast<int>(std::upper_bound(e0.begin(), e0.end(), e) - e0.begin()) - 1;
+  };
   // hit[j][c]: chunk c holds a face neighbour of an element of chunk j, or
   // the other way round (the relation is made symmetric, so that every
   // chunk that reads a chunk's stage input in stage g precedes that chunk's
   // stage g + 2, which overwrites its q0 in stage 3).
-  std::vector<std::vector<char>> hit(S, std::vector<char>(S, 0));
-  for (int j = 0; j < S; ++j) {
-    hit[j][j] = 1;
-    for (int e = e0[j]; e < e0[j + 1]; ++e)
-      for (int f = 0; f < 6; ++f) {
-        const int p = pb[6 * static_cast<size_t>(e) + f];
-        if (p < 0) return SDG_OK;  // a halo face: no pipelining
-        const int ne = p / h->Np;
-        const int c =
-            static_cast<int>(std::upper_bound(e0.begin(), e0.end(), ne) - e0.begin()) - 1;
-        hit[j][c] = hit[c][j] = 1;
-      }
-  }
-  std::vector<std::vector<int>> nbr(S);
-  for (int j = 0; j < S; ++j)
-    for (int c = 0; c < S; ++c)
-      if (hit[j][c]) nbr[j].push_back(c);
+  auto neighbours = [&](const int* dpb, bool halo_ok, std::vector<std::vector<int>>* nbr,
+                        std::vector<char>* halo) -> bool {
+    std::vector<int> pb(6 * static_cast<size_t>(h->Ne));
+    if (cudaMemcpy(pb.data(), dpb, pb.size() * sizeof(int), cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+      return false;
+    std::vector<std::vector<char>> hit(S, std::vector<char>(S, 0));
+    halo->assign(S, 0);
+    for (int j = 0; j < S; ++j) {
+      hit[j][j] = 1;
+      for (int e = e0[j]; e < e0[j + 1]; ++e)
+        for (int f = 0; f < 6; ++f) {
+          const int p = pb[6 * static_cast<size_t>(e) + f];
+          if (p < 0) {
+            if (!halo_ok) return false;
+            (*halo)[j] = 1;
+            continue;
+          }
+          const int c = chunk_of(p / h->Np);
+          hit[j][c] = hit[c][j] = 1;
+        }
+    }
+    nbr->assign(S, {});
+    for (int j = 0; j < S; ++j)
+      for (int c = 0; c < S; ++c)
+        if (hit[j][c]) (*nbr)[j].push_back(c);
+    return true;
+  };
+  std::vector<std::vector<int>> nbr, nbr_h;
+  std::vector<char> unused, halo;
+  if (!neighbours(h->pb_halo, true, &nbr_h, &halo))
+    return fail(SDG_ERR_CUDA, "reading the face-neighbour table failed");
+  if (!h->direct_ok || !neighbours(h->pb_direct, false, &nbr, &unused)) nbr.clear();
   if (!h->copy_in) {
     SDG_CUDA(cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
     SDG_CUDA(cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
@@ -611,7 +635,87 @@ int build_chunks(sdg_handle* h) {
   }
   h->chunk_e0 = e0;
   h->chunk_nbr = nbr;
+  h->chunk_nbr_h = nbr_h;
+  h->chunk_halo = halo;
   return SDG_OK;
+}
+
+// sdg_cal_tend by element chunks: the halo parts of q, u, v, w go up first,
+// then the chunks in order on copy_in; each chunk's tendency starts once the
+// chunks it reads are up, and its dqdt goes back on copy_out as soon as it
+// is computed, so the copies overlap each other and the kernels.
+int cal_tend_chunked(sdg_handle* h, double* dqdt, const double* const src[4]) {
+  const int S = static_cast<int>(h->chunk_e0.size()) - 1;
+  const size_t Np = static_cast<size_t>(h->Np);
+  const size_t NE = Np * h->Ne, NA = Np * h->NeA;
+  cudaEvent_t ek0, ek1;
+  SDG_CUDA(cudaEventCreate(&ek0));
+  SDG_CUDA(cudaEventCreate(&ek1));
+  SDG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  SDG_CUDA(cudaEventRecord(h->ev_in, h->stream));
+  SDG_CUDA(cudaStreamWaitEvent(h->copy_in, h->ev_in, 0));
+  SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_in, 0));
+  if (NA > NE)
+    for (int i = 0; i < 4; ++i)
+      SDG_CUDA(cudaMemcpyAsync(h->io[i] + NE, src[i] + NE, (NA - NE) * sizeof(double),
+                               cudaMemcpyHostToDevice, h->copy_in));
+  for (int j = 0; j < S; ++j) {
+    const size_t a = h->chunk_e0[j] * Np, n = (h->chunk_e0[j + 1] - h->chunk_e0[j]) * Np;
+    for (int i = 0; i < 4; ++i)
+      SDG_CUDA(cudaMemcpyAsync(h->io[i] + a, src[i] + a, n * sizeof(double),
+                               cudaMemcpyHostToDevice, h->copy_in));
+    SDG_CUDA(cudaEventRecord(h->ev_up[j], h->copy_in));
+  }
+  // Chunk j needs the uploads up to the last chunk it reads (the halo went
+  // first); chunks go in the order their inputs arrive.
+  std::vector<std::pair<int, int>> order(S);
+  for (int j = 0; j < S; ++j) order[j] = {h->chunk_nbr_h[j].back(), j};
+  std::stable_sort(order.begin(), order.end());
+  int waited = -1, rc = SDG_OK;
+  for (int k = 0; k < S && !rc; ++k) {
+    const int need = order[k].first, j = order[k].second;
+    if (need > waited) {
+      SDG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_up[need], 0));
+      waited = need;
+    }
+    if (k == 0) SDG_CUDA(cudaEventRecord(ek0, h->stream));
+    LaunchSpec s = base_spec(h, false);
+    s.kind = kTendF64;
+    s.q = h->io[0];
+    s.u = h->io[1];
+    s.v = h->io[2];
+    s.w = h->io[3];
+    s.out = h->io[4];
+    s.pbase = h->pb_halo;
+    s.elem0 = h->chunk_e0[j];
+    s.nelem = h->chunk_e0[j + 1] - h->chunk_e0[j];
+    rc = launch_tend(s);
+    if (rc) break;
+    ++h->launches;
+    const size_t a = s.elem0 * Np, n = s.nelem * Np;
+    SDG_CUDA(cudaEventRecord(h->ev_fin[j], h->stream));
+    SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_fin[j], 0));
+    SDG_CUDA(cudaMemcpyAsync(dqdt + a, h->io[4] + a, n * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->copy_out));
+  }
+  cudaEventRecord(ek1, h->stream);
+  cudaEventRecord(h->ev_out, h->copy_out);
+  cudaStreamWaitEvent(h->stream, h->ev_out, 0);
+  cudaEventRecord(h->ev1, h->stream);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (!rc && e != cudaSuccess)
+    rc = fail(SDG_ERR_CUDA, "sdg_cal_tend: %s", cudaGetErrorString(e));
+  if (!rc) rc = check_status(h);
+  if (!rc) {
+    float all = 0, kern = 0;
+    cudaEventElapsedTime(&all, h->ev0, h->ev1);
+    cudaEventElapsedTime(&kern, ek0, ek1);
+    h->t_tend += 1e-3 * kern;
+    h->t_copy += 1e-3 * (all - kern);
+  }
+  cudaEventDestroy(ek0);
+  cudaEventDestroy(ek1);
+  return rc;
 }
 
 // Enqueues the three stages of one RK3 step chunk by chunk on the handle's
@@ -826,6 +930,8 @@ int sdg_cal_tend(sdg_handle* h, double* dqdt, const double* q,
     if (!h->io[i] && !(h->io[i] = dev_alloc<double>(NA, &rc))) return rc;
   const double* src[4] = {q, u, v, w};
   account_rk(h);
+  if ((rc = build_chunks(h))) return rc;
+  if (!h->chunk_nbr_h.empty()) return cal_tend_chunked(h, dqdt, src);
   cudaEvent_t e2, e3;
   SDG_CUDA(cudaEventCreate(&e2));
   SDG_CUDA(cudaEventCreate(&e3));
@@ -941,7 +1047,7 @@ int sdg_rk3_steps_host(sdg_handle* h, double* q, double dt, int nsteps) {
                 "stages; run sdg_update_halo_stage, the exchange and sdg_rk3_stage");
   if ((rc = ensure_state(h))) return rc;
   if ((rc = build_chunks(h))) return rc;
-  if (h->chunk_e0.empty() || nsteps == 0) {
+  if (h->chunk_nbr.empty() || nsteps == 0) {
     if ((rc = sdg_set_field(h, SDG_FIELD_Q, q))) return rc;
     if ((rc = sdg_rk3_steps(h, dt, nsteps))) return rc;
     return sdg_get_field(h, SDG_FIELD_Q, q);

@@ -1,5 +1,6 @@
-"""sdg_rk3_steps_host: the pipelined host-buffer RK call equals
-sdg_set_field + sdg_rk3_steps + sdg_get_field bit for bit (needs a B200).
+"""The chunked host-buffer calls (needs a B200): sdg_rk3_steps_host equals
+sdg_set_field + sdg_rk3_steps + sdg_get_field bit for bit, and sdg_cal_tend
+on host arrays equals sdg_cal_tend_dev on the same arrays in device memory.
 
 The call cuts the element range into chunks (runs of z-layers in a box)
 and runs the first and last steps chunk by chunk while the state's chunks
@@ -107,3 +108,28 @@ def test_host_steps_argument_errors():
     h.rk3_steps_host(q, dt, 0)              # upload and download only
     assert np.array_equal(q, fields[0][:, : mesh.Ne])
     h.close()
+
+
+@pytest.mark.parametrize("dims,p,flags", [
+    ((16, 16, 8), 1, sdg.FLAG_EXACT),
+    ((13, 16, 20), 2, 0),
+    ((12, 12, 16), 7, 0),
+])
+def test_chunked_tendency_call_equals_device_call(dims, p, flags):
+    """sdg_cal_tend on host arrays (meshes of 2,048+ elements: the copies
+    and the tendency run by element chunks) equals sdg_cal_tend_dev on the
+    same arrays in device memory, including a halo buffer that does not
+    match the periodic neighbours (both read it where VMapP points)."""
+    ops, mesh, fields, dt = make(dims, p, flags)
+    q, u, v, w = (np.array(a, order="F") for a in fields)
+    halo = slice(mesh.Ne, mesh.NeA)
+    q[:, halo] *= 0.5            # a stale halo: the call must still read it
+    h = sdg.Handle(ops, mesh, flags)
+    got = h.cal_tend(q, u, v, w)[:, : mesh.Ne]
+    dev = [torch.from_numpy(a.reshape(-1, order="F")).cuda() for a in (q, u, v, w)]
+    out = torch.zeros_like(dev[0])
+    h.cal_tend_dev(out, *dev)
+    torch.cuda.synchronize()
+    ref = out.cpu().numpy().reshape(mesh.Np, mesh.NeA, order="F")[:, : mesh.Ne]
+    h.close()
+    assert np.array_equal(got, ref)
