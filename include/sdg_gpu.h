@@ -157,7 +157,11 @@ int sdg_finalize(sdg_handle* h);
 /* Drop-in for advect3d_eq_cal_tend (mod_advect3d_eq.f90:41-85) on host
  * arrays q,u,v,w(Np,NeA) (halo filled by the caller, as the reference
  * reads it through VMapP) -> dqdt(Np,NeA), of which (:,1:Ne) is written.
- * Copies in, runs the fused kernel, copies out; synchronous. */
+ * Copies in, runs the fused kernel, copies out; synchronous.  Meshes of
+ * 2,048+ elements go by element chunks (the halo parts first), each
+ * chunk's kernel starting once the chunks it reads are up and its dqdt
+ * going back at once, so the copies overlap (host arrays pinned for that);
+ * the result equals sdg_cal_tend_dev on the same arrays. */
 int sdg_cal_tend(sdg_handle* h, double* dqdt, const double* q,
                  const double* u, const double* v, const double* w);
 
