@@ -30,11 +30,25 @@
 
 namespace sdg {
 
+// Orders whose column parts each take a whole number of warps (Nq^2 threads
+// rounded up to a multiple of 32, the rest idle), so that no warp holds
+// threads of both parts and every phase is one pass per warp (the warp that
+// straddles the parts otherwise contracts both an x and a y line and
+// evaluates both kinds of face).  Measured (RK stage 2, ~16.8 M DOF, ms
+// padded / not): FP64 p = 8 0.223 / 0.253, p = 11 0.251 / 0.291, p = 12
+// 0.246 / 0.273; mixed p = 8 0.129 / 0.149, p = 11 0.132 / 0.142.  Slower
+// at FP64 p = 9 (0.274 / 0.223: a whole warp more for four columns) and
+// p = 13 (0.267 / 0.252: 132 bytes of spill at 448 threads).
+template <int NQ>
+constexpr bool kSplitPadParts = NQ == 9 || NQ == 11 || NQ == 12 || NQ == 13 || NQ == 15;
+
 template <int NQ, int H>
 struct SplitGeo {
   static constexpr int NQ2 = NQ * NQ;
   static constexpr int NP = NQ2 * NQ;
-  static constexpr int THREADS = H * NQ2;
+  static constexpr bool PAD = kSplitPadParts<NQ>;
+  static constexpr int PT = PAD ? (NQ2 + 31) / 32 * 32 : NQ2;  // threads per part
+  static constexpr int THREADS = H * PT;
   static constexpr int KZ = (NQ + H - 1) / H;  // column nodes per thread
 };
 
@@ -105,7 +119,7 @@ struct SplitPlan {
   }
   // Resident blocks the registers allow (kSplitRegFloor registers a thread).
   static constexpr int REG_BLOCKS =
-      65536 / (((H * NQ2 + 31) / 32 * 32) * kSplitRegFloor<NQ, TC>);
+      65536 / (((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32) * kSplitRegFloor<NQ, TC>);
   static constexpr int cap(int b) { return b < REG_BLOCKS ? b : REG_BLOCKS; }
   // The most resident blocks any layout reaches, and the first layout that
   // reaches it in the order of preference: separate line buffers, then q0
@@ -174,14 +188,15 @@ constexpr int kSplitH = 2;
 
 // Where the automatic variant takes the split-column kernel: the orders at
 // which it measured faster than tend_pipe_kernel (RK stage 2, ~16.8 M DOF,
-// ms split / pipelined): fast FP64 p = 8 0.255 / 0.263, p = 9 0.226 / 0.254,
-// p = 11 0.290 / 0.327, p = 12 0.274 / 0.319, p = 13 0.256 / 0.299; mixed
-// p = 9 0.143 / 0.159, p = 11 0.142 / 0.148.  Slower at FP64 p = 10 and 14
-// (0.244 / 0.233, 0.332 / 0.313) and the other mixed orders.
+// ms split / pipelined): fast FP64 p = 8 0.223 / 0.261, p = 9 0.223 / 0.253,
+// p = 11 0.251 / 0.325, p = 12 0.246 / 0.316, p = 13 0.252 / 0.295; mixed
+// p = 8 0.129 / 0.146, p = 9 0.144 / 0.158, p = 11 0.132 / 0.146.  Slower at
+// FP64 p = 10 and 14 (0.232 / 0.230, 0.332 / 0.313) and the other mixed
+// orders.
 template <int NQ, typename TC, bool EXACT>
 constexpr bool kSplitAuto =
     !EXACT && (sizeof(TC) == 8 ? (NQ == 9 || NQ == 10 || (NQ >= 12 && NQ <= 14))
-                               : (NQ == 10 || NQ == 12));
+                               : (NQ == 9 || NQ == 10 || NQ == 12));
 
 // Blocks per SM the kernel is built for: what the shared memory allows,
 // capped so that a thread keeps at least kSplitRegFloor registers.
@@ -223,20 +238,22 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
   uint64_t* bars = reinterpret_cast<uint64_t*>(rest + P::FACE + FLUXB + P::LIFTB);
   constexpr bool SEP = P::SEP;
 
-  const int h = threadIdx.x / NQ2;      // part of the column
-  const int c = threadIdx.x - h * NQ2;  // column a + NQ*b
+  constexpr int PT = G::PT;
+  const int h = threadIdx.x / PT;       // part of the column
+  const int c = threadIdx.x - h * PT;   // column a + NQ*b
+  const bool valid = !G::PAD || c < NQ2;  // padded parts: idle beyond Nq^2
   const int a = c % NQ;
   const int b = c / NQ;
   const int k0 = h * KZ;                // first node of this thread's part
   const int ntiles = BATCH ? A.ntiles : A.nelem;
-  const bool own_y = h == 0;            // y faces and the -z face
-  const bool own_x = h == H - 1;        // x faces and the +z face
+  const bool own_y = h == 0 && valid;      // y faces and the -z face
+  const bool own_x = h == H - 1 && valid;  // x faces and the +z face
   const unsigned spins = A.wait_spins;
   // The part of this warp's threads, or -1 when the warp holds both.
   auto part_of_warp = [&]() {
     const int t0 = threadIdx.x & ~31;
     const int t1 = min(t0 + 31, static_cast<int>(blockDim.x) - 1);
-    return (t0 / NQ2 == t1 / NQ2) ? t0 / NQ2 : -1;
+    return (t0 / PT == t1 / PT) ? t0 / PT : -1;
   };
 
   // Minus-side face values (FaceArea): FP64 keeps the x faces in two scalar
@@ -399,7 +416,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     const bool use_q0 = STAGE && A.rk_a != 0.0;
     auto load_q0 = [&]() {
       if constexpr (STAGE && !P::RING_Q0) {
-        if (use_q0) {
+        if (use_q0 && valid) {
 #pragma unroll
           for (int kk = 0; kk < KZ; ++kk) {
             const int k = k0 + kk;
@@ -462,12 +479,14 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         if (ony) fmy[NQ * k] = V2{qv, vv};
       }
     };
-    if (hw < 0)
+    if (!valid) {
+    } else if (hw < 0) {
       phase1(Part<-1>{});
-    else if (hw == 0)
+    } else if (hw == 0) {
       phase1(Part<0>{});
-    else
+    } else {
       phase1(Part<1>{});
+    }
     // The slot's writes (q*w; line buffers in u, v without SEP) come before
     // the refill that overwrites it.
     fence_proxy_async_smem();
@@ -477,7 +496,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
 #pragma unroll
       for (int kk = 0; kk < KZ; ++kk) {
         const int k = k0 + kk;
-        if (KZ * H != NQ && k >= NQ) break;
+        if ((KZ * H != NQ && k >= NQ) || !valid) break;
         sX[LI::colx(a, b, k)] = fx[kk];
         sY[LI::coly(a, b, k)] = fy[kk];
       }
@@ -487,7 +506,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
     // ---- Lines: x-line c (h = 0) and y-line c (h = 1), in place ----------
     {
       const int lbx = LI::xl_base(a, b), lby = LI::yl_base(a, b);
-      if (h == 0) {
+      if (h == 0 && valid) {
         TC line[NQ];
 #pragma unroll
         for (int l = 0; l < NQ; ++l) line[l] = sX[LI::xl(lbx, l)];
@@ -496,7 +515,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
           sX[LI::xl(lbx, i)] = contract<NQ, ORDER, AR, TC>(
               [&](int l) { return D.d[i * NQ + l]; }, [&](int l) { return line[l]; });
       }
-      if (h == H - 1) {
+      if (h == H - 1 && valid) {
         TC line[NQ];
 #pragma unroll
         for (int l = 0; l < NQ; ++l) line[l] = sY[LI::yl(lby, l)];
@@ -626,12 +645,14 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         }
       }
     };
-    if (hw < 0)
+    if (!valid) {
+    } else if (hw < 0) {
       epilogue(Part<-1>{});
-    else if (hw == 0)
+    } else if (hw == 0) {
       epilogue(Part<0>{});
-    else
+    } else {
       epilogue(Part<1>{});
+    }
   }
 }
 
