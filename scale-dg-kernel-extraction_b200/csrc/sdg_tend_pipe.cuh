@@ -324,7 +324,14 @@ struct FaceArea {
   static constexpr int XOFF = NQ2 + 4;
   static constexpr int XA = 2 * XOFF;                // one x array (q or u)
   static constexpr int Y0 = SPLIT ? 2 * XA : 4 * NQ2;  // start of the y pairs
-  static constexpr int ELEM = Y0 + 4 * NQ2;
+  // Pairs (SPLIT = false): the -x block starts P3 pairs after 3 Nq^2, so that
+  // the threads of a warp on the -x face (a = 0) and on the +x face
+  // (a = Nq-1) store their (q, u) pairs 16 banks apart, not on the same ones.
+  static constexpr int P3 = SPLIT ? 0 : ((8 - 2 * NQ2) % 16 + 16) % 16;
+  static constexpr int F3 = 3 * NQ2 + P3;            // pair index of the -x block
+  static constexpr int ELEM = SPLIT ? Y0 + 4 * NQ2 : 2 * (4 * NQ2 + P3);
+  // Pair index of face block f (0: -y, 1: +x, 2: +y, 3: -x).
+  static __host__ __device__ constexpr int block(int f) { return f == 3 ? F3 : f * NQ2; }
 };
 
 // Thread geometry: Nq^2 threads per element, EPB elements per block
@@ -780,7 +787,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
       const bool onx = (a == 0) || (a == NQ - 1);
       const bool ony = (b == 0) || (b == NQ - 1);
       const int xo = (a == 0 ? FA::XOFF : 0) + b;
-      V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
+      V2* fmx = fM + (a == 0 ? FA::F3 : NQ2) + b;
       V2* fmy = XSPLIT ? ypair + (b == 0 ? 0 : NQ2) + a : fM + (b == 0 ? 0 : 2) * NQ2 + a;
 #pragma unroll
       for (int k = 0; k < NQ; ++k) {
@@ -877,7 +884,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
                 unP[f] = m.y;
               }
             } else {
-              const V2 m = reinterpret_cast<const V2*>(nfa)[((f + 2) & 3) * NQ2 + t];
+              const V2 m = reinterpret_cast<const V2*>(nfa)[FA::block((f + 2) & 3) + t];
               qP[f] = m.x;
               unP[f] = m.y;
             }
@@ -994,7 +1001,7 @@ __global__ void __launch_bounds__((PipeGeo<NQ>::THREADS + 31) / 32 * 32,
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
           const TC sg = (f == 0 || f == 3) ? TC(-1) : TC(1);
-          const V2 m = fM[f * NQ2 + t];
+          const V2 m = fM[FA::block(f) + t];
           fl[f] = upwind_flux<AR, TC>(m.x, m.y, qP[f], unP[f], sg, sfs[f]);
         }
         fM[t] = V2{fl[0], fl[2]};

@@ -274,7 +274,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
   V2* fl13 = FAL ? (XSPLIT ? ypair : fM) : reinterpret_cast<V2*>(flux);
   V2* fl24 = FAL ? fM + NQ2 : reinterpret_cast<V2*>(flux) + NQ2;
   TC* fl5 = FAL ? reinterpret_cast<TC*>(XSPLIT ? ypair + NQ2 : fM + 2 * NQ2) : flux + 4 * NQ2;
-  TC* fl6 = FAL ? (XSPLIT ? xu : reinterpret_cast<TC*>(fM + 3 * NQ2)) : flux + 5 * NQ2;
+  TC* fl6 = FAL ? (XSPLIT ? xu : reinterpret_cast<TC*>(fM + FA::F3)) : flux + 5 * NQ2;
   // Word stride of f5 and f6 between columns (pairs in the aliased form).
   constexpr int S5 = FAL ? 2 : 1;
   constexpr int S6 = (FAL && !XSPLIT) ? 2 : 1;
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
       const bool onx = (a == 0) || (a == NQ - 1);
       const bool ony = (b == 0) || (b == NQ - 1);
       [[maybe_unused]] const int xo = (a == 0 ? FA::XOFF : 0) + b;
-      [[maybe_unused]] V2* fmx = fM + (a == 0 ? 3 : 1) * NQ2 + b;
+      [[maybe_unused]] V2* fmx = fM + (a == 0 ? FA::F3 : NQ2) + b;
       V2* fmy = XSPLIT ? ypair + (b == 0 ? 0 : NQ2) + a : fM + (b == 0 ? 0 : 2) * NQ2 + a;
 #pragma unroll
       for (int kk = 0; kk < KZ; ++kk) {
@@ -557,7 +557,7 @@ __global__ void __launch_bounds__((SplitGeo<NQ, H>::THREADS + 31) / 32 * 32,
         q4 = xq[FA::XOFF + xn];
         u4 = xu[FA::XOFF + xn];
       } else {
-        const V2 m2 = fM[NQ2 + c], m4 = fM[3 * NQ2 + c];
+        const V2 m2 = fM[NQ2 + c], m4 = fM[FA::F3 + c];
         q2 = m2.x;
         u2 = m2.y;
         q4 = m4.x;
