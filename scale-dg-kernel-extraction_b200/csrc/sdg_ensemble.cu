@@ -25,6 +25,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -520,24 +521,48 @@ struct Ensemble {
   // Times the candidate tile shapes of each group on its current members
   // (RK stage 2, which reads q1 and q0 and writes q2; q2 is rewritten by
   // every real step before it is read) and keeps the fastest.
+  // The kernel variants a group's launches support.
+  std::vector<int> candidates(const Group* g) const {
+    std::vector<int> cands;
+    const bool can_pipe = pipe_supported(g->nq, g->mixed ? kStageMixed2 : kStageF64) &&
+                          pipe_supported(g->nq, g->mixed ? kStageMixed1 : kStageF64) &&
+                          pipe_supported(g->nq, g->mixed ? kStageMixed3 : kStageF64);
+    if (can_pipe) cands.push_back(kVariantPipe);
+    const bool can_split = split_supported(g->nq, g->mixed ? kStageMixed2 : kStageF64) &&
+                           split_supported(g->nq, g->mixed ? kStageMixed1 : kStageF64) &&
+                           split_supported(g->nq, g->mixed ? kStageMixed3 : kStageF64) &&
+                           ((g->flags & SDG_FLAG_EXACT) || !g->ops->lift_z.empty());
+    if (can_split) cands.push_back(kVariantSplit);
+    cands.push_back(kVariantBlock);
+    if (g->nq >= 4 && g->nq <= 8) cands.push_back(kVariantBlockOcc);
+    return cands;
+  }
+
+  // SDG_KERNEL=block|pipe|blockocc|split, as for a handle: every group whose
+  // order supports that variant takes it in place of the autotuner's choice.
+  void force_variant() {
+    const char* kv = std::getenv("SDG_KERNEL");
+    if (!kv) return;
+    int v = -1;
+    if (std::strcmp(kv, "block") == 0) v = kVariantBlock;
+    else if (std::strcmp(kv, "pipe") == 0) v = kVariantPipe;
+    else if (std::strcmp(kv, "blockocc") == 0) v = kVariantBlockOcc;
+    else if (std::strcmp(kv, "split") == 0) v = kVariantSplit;
+    if (v < 0) return;
+    for (auto& kvp : groups) {
+      Group* g = kvp.second.get();
+      const std::vector<int> c = candidates(g);
+      if (std::find(c.begin(), c.end(), v) != c.end()) g->variant = v;
+    }
+  }
+
   int autotune(int reps) {
     for (auto& kv : groups) {
       Group* g = kv.second.get();
       if (g->members.empty()) continue;
       int rc = rebuild(g);
       if (rc) return rc;
-      std::vector<int> cands;
-      const bool can_pipe = pipe_supported(g->nq, g->mixed ? kStageMixed2 : kStageF64) &&
-                            pipe_supported(g->nq, g->mixed ? kStageMixed1 : kStageF64) &&
-                            pipe_supported(g->nq, g->mixed ? kStageMixed3 : kStageF64);
-      if (can_pipe) cands.push_back(kVariantPipe);
-      const bool can_split = split_supported(g->nq, g->mixed ? kStageMixed2 : kStageF64) &&
-                             split_supported(g->nq, g->mixed ? kStageMixed1 : kStageF64) &&
-                             split_supported(g->nq, g->mixed ? kStageMixed3 : kStageF64) &&
-                             ((g->flags & SDG_FLAG_EXACT) || !g->ops->lift_z.empty());
-      if (can_split) cands.push_back(kVariantSplit);
-      cands.push_back(kVariantBlock);
-      if (g->nq >= 4 && g->nq <= 8) cands.push_back(kVariantBlockOcc);
+      const std::vector<int> cands = candidates(g);
       cudaEvent_t e0, e1;
       ENS_CUDA(cudaEventCreate(&e0));
       ENS_CUDA(cudaEventCreate(&e1));
@@ -713,6 +738,7 @@ int sdg_batch_commit(sdg_batch* b, int autotune) {
   cudaSetDevice(b->ens.dev);
   int rc;
   if (autotune && (rc = b->ens.autotune(5))) return rc;
+  b->ens.force_variant();
   if ((rc = b->ens.prime())) return rc;
   if ((rc = capture_step(b))) return rc;
   ENS_CUDA(cudaEventCreate(&b->ev0));

@@ -62,6 +62,40 @@ def test_batch_equals_single_instances(flags):
     b.close()
 
 
+HIGH_CASES = [(8, (2, 3, 2), 11), (9, (2, 2, 3), 12), (10, (2, 2, 2), 13), (11, (3, 2, 2), 14),
+              (12, (2, 2, 2), 15), (13, (2, 2, 1), 16), (14, (2, 1, 2), 17)]
+
+
+@pytest.mark.parametrize("variant", ["split", "pipe", "block"])
+@pytest.mark.parametrize("flags", [0, sdg.FLAG_MIXED])
+def test_forced_batch_variant_equals_single_instances(variant, flags, monkeypatch):
+    """SDG_KERNEL forces one kernel variant on every group of a batch whose
+    order supports it: the batched split-column kernel (whole-warp parts at
+    p = 8, 10-12 and 14, q0 through the ring where the plan holds it, the
+    tile context in the slot), the batched pipelined kernel and the
+    one-tile-per-block kernel all reproduce the single instances bit for
+    bit at p = 8..14."""
+    monkeypatch.setenv("SDG_KERNEL", variant)
+    nstep = 3
+    b = sdg.Batch(flags)
+    insts = [instance(p, dims, seed) for p, dims, seed in HIGH_CASES]
+    ids = [b.add(*dims, p, ops, *fields, dt) for (p, dims, _), (ops, mesh, fields, dt)
+           in zip(HIGH_CASES, insts)]
+    b.commit(autotune=False)
+    b.run(nstep)
+    names = {1: "block", 2: "pipe", 3: "blockocc", 4: "split"}
+    chosen = {g["p"]: names.get(g["variant"]) for g in b.info()["groups"]}
+    if variant in ("pipe", "block"):
+        assert all(v == variant for v in chosen.values()), chosen
+    else:
+        assert sum(v == "split" for v in chosen.values()) >= 5, chosen
+    monkeypatch.delenv("SDG_KERNEL")
+    for i, (ops, mesh, fields, dt) in zip(ids, insts):
+        want = single_run(ops, mesh, fields, dt, nstep, flags)
+        assert np.array_equal(b.get(i), want), i
+    b.close()
+
+
 def test_exact_batch_equals_oracle():
     nstep = 4
     b = sdg.Batch(sdg.FLAG_EXACT)
