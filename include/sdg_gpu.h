@@ -297,7 +297,10 @@ int sdg_batch_add(sdg_batch* b, int NeX, int NeY, int NeZ, int p,
  * is one persistent launch over a tile table; with autotune != 0 each
  * group's tile shape (kernel variant: elements per block x nodes per
  * thread) is chosen by timing the candidates on the group's instances.
- * One RK step of all groups is captured as a CUDA graph. */
+ * The environment variable SDG_KERNEL=block|pipe|blockocc|split, when set,
+ * overrides the choice for every group whose order supports that variant.
+ * One RK step of all groups is captured as a CUDA graph; its groups run one
+ * after another. */
 int sdg_batch_commit(sdg_batch* b, int autotune);
 
 /* Advances every instance by nsteps SSP-RK3 steps (graph replays);
