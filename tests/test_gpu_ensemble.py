@@ -67,14 +67,14 @@ HIGH_CASES = [(8, (2, 3, 2), 11), (9, (2, 2, 3), 12), (10, (2, 2, 2), 13), (11, 
 
 
 @pytest.mark.parametrize("variant", ["split", "pipe", "block"])
-@pytest.mark.parametrize("flags", [0, sdg.FLAG_MIXED])
+@pytest.mark.parametrize("flags", [0, sdg.FLAG_MIXED, sdg.FLAG_EXACT])
 def test_forced_batch_variant_equals_single_instances(variant, flags, monkeypatch):
     """SDG_KERNEL forces one kernel variant on every group of a batch whose
     order supports it: the batched split-column kernel (whole-warp parts at
     p = 8, 10-12 and 14, q0 through the ring where the plan holds it, the
     tile context in the slot), the batched pipelined kernel and the
     one-tile-per-block kernel all reproduce the single instances bit for
-    bit at p = 8..14."""
+    bit at p = 8..14, in the fast FP64, mixed and exact forms."""
     monkeypatch.setenv("SDG_KERNEL", variant)
     nstep = 3
     b = sdg.Batch(flags)
