@@ -193,14 +193,16 @@ int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps);
 /* sdg_set_field(SDG_FIELD_Q, q) + sdg_rk3_steps(dt, nsteps) +
  * sdg_get_field(SDG_FIELD_Q, q) in one call, with the same result bit for
  * bit: q (Np,Ne) FP64 on the host in, the state after nsteps steps back in
- * q.  The element range is cut into up to 16 chunks (runs of z-layers in a
- * box) and the first step's stages run chunk by chunk as soon as the
- * chunks they read are uploaded, the last step's as the state's chunks go
- * back, so the two copies and the stages overlap (host memory pinned with
- * cudaHostAlloc / cudaHostRegister for the copies to run asynchronously).
- * Meshes of fewer than 2,048 elements, or whose boundary faces read the
- * halo buffer, take the three calls in order.  Velocities must be set
- * (sdg_set_field).  Synchronises the handle. */
+ * q.  The element range is cut into chunks (runs of z-layers in a box;
+ * one layer thin at both ends) and the first step's stages run chunk by
+ * chunk as soon as the chunks they read are uploaded, the last step's as
+ * the state's chunks go back, so the two copies and the stages overlap
+ * (host memory pinned with cudaHostAlloc / cudaHostRegister for the copies
+ * to run asynchronously; a one-step call on pinned memory replays a CUDA
+ * graph captured for that array and dt).  Meshes of fewer than 2,048
+ * elements (fewer than 4 chunks of 512 elements or 2^18 nodes), or whose
+ * boundary faces read the halo buffer, take the three calls in order.
+ * Velocities must be set (sdg_set_field).  Synchronises the handle. */
 int sdg_rk3_steps_host(sdg_handle* h, double* q, double dt, int nsteps);
 
 /* min/max of q(:,1:Ne) (main.f90:76-79); synchronises the handle. */

@@ -234,6 +234,13 @@ struct sdg_handle {
   // Step graph.
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0.0;
+  // Graph of one sdg_rk3_steps_host step (uploads, chunked stages and
+  // downloads) for the pinned host array host_graph_q and host_graph_dt,
+  // and the number of kernels it launches.
+  cudaGraphExec_t host_graph = nullptr;
+  const double* host_graph_q = nullptr;
+  double host_graph_dt = 0.0;
+  long long host_graph_launches = 0;
 
   // sdg_rk3_steps_host and sdg_cal_tend (lazy): element chunks (boundaries,
   // S + 1 of them; empty when the mesh is too small to pipeline), each
@@ -263,6 +270,7 @@ void free_handle(sdg_handle* h) {
   cudaSetDevice(h->dev);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->host_graph) cudaGraphExecDestroy(h->host_graph);
   void* ptrs[] = {h->lift64, h->lift32, h->pb_halo, h->pb_direct, h->esc64,
                   h->esc32,  h->fsc64,  h->fsc32,   h->hsrc,      h->io[0],
                   h->io[1],  h->io[2],  h->io[3],   h->io[4],     h->q0,
@@ -561,26 +569,82 @@ int ensure_graph(sdg_handle* h, double dt) {
   return SDG_OK;
 }
 
+// Releases the graphs (they hold kernel arguments: variant, test hooks).
+void drop_graphs(sdg_handle* h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->host_graph) cudaGraphExecDestroy(h->host_graph);
+  h->graph = nullptr;
+  h->host_graph = nullptr;
+  h->host_graph_q = nullptr;
+}
+
 // Element chunks of sdg_rk3_steps_host and sdg_cal_tend: S contiguous
-// element ranges (at most 16, at least 512 elements each; fewer than 4
-// chunks do not pipeline) and, per chunk, the chunks that hold a face
-// neighbour of one of its elements, through the direct table (the RK path;
-// it does not pipeline when a boundary face reads the halo buffer) and
-// through the halo table (the tendency call, which reads the caller's
-// halo).  Elements are
-// numbered x fastest, so in a box each chunk is a run of z-layers and its
-// neighbours are the chunks before and after it (cyclically).  The chunk
-// count trades the tail (the last upload's neighbours, about six chunks,
-// finish and go back after it) against the two copies' overlap, which slows
-// both directions: FP64 32^3 p = 7, one step, 4.37 / 4.24 / 4.79 ms with
-// 32 / 16 / 8 chunks (the three calls 5.31 ms).
+// element ranges (fewer than 4 chunks do not pipeline) and, per chunk, the
+// chunks that hold a face neighbour of one of its elements, through the
+// direct table (the RK path; it does not pipeline when a boundary face
+// reads the halo buffer) and through the halo table (the tendency call,
+// which reads the caller's halo).  Elements are numbered x fastest, so in a
+// box each chunk is a run of z-layers and its neighbours are the chunks
+// before and after it (cyclically).  The last upload's chunk and its
+// neighbours to a depth of three finish after it and go back last, so the
+// three first and four last chunks are one z-layer thin and the chunks
+// between them about Ne/16.  One step from pinned memory (ms; the three
+// calls 5.31 at FP64 32^3 p = 7):
+//
+//   chunks                       FP64 32^3 p7   mixed 32^3 p7   mixed 16^3 p15
+//   16 equal                     4.17           4.10            4.71 (8 equal)
+//   32 equal                     4.32           4.16            -
+//   7 thin + 6 of Ne/8           4.24           4.21            -
+//   7 thin + 13 of Ne/16         3.97           3.93            4.18
+//
+// The copies in the two directions share the bus: alone 55 / 52 GB/s, both
+// at once 43 GB/s each (134 MB each way in 3.15 ms).
 int build_chunks(sdg_handle* h) {
   if (h->chunks_built) return SDG_OK;
   h->chunks_built = true;
-  const int S = std::min(16, h->Ne / 512);
-  if (S < 4) return SDG_OK;
-  std::vector<int> e0(S + 1);
-  for (int j = 0; j <= S; ++j) e0[j] = static_cast<int>(static_cast<long>(h->Ne) * j / S);
+  const int Ne = h->Ne;
+  const size_t Np = static_cast<size_t>(h->Np);
+  std::vector<int> pbh(6 * static_cast<size_t>(Ne)), pbd;
+  if (cudaMemcpy(pbh.data(), h->pb_halo, pbh.size() * sizeof(int), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return fail(SDG_ERR_CUDA, "reading the face-neighbour table failed");
+  if (h->direct_ok) {
+    pbd.resize(pbh.size());
+    if (cudaMemcpy(pbd.data(), h->pb_direct, pbd.size() * sizeof(int),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(SDG_ERR_CUDA, "reading the face-neighbour table failed");
+  }
+  // Reach: the largest cyclic index distance between an element and a face
+  // neighbour (a z-layer, NeX * NeY, in a periodic box).
+  int reach = 1;
+  for (int e = 0; e < Ne; ++e)
+    for (int f = 0; f < 6; ++f) {
+      const int p = pbh[6 * static_cast<size_t>(e) + f];
+      if (p < 0) continue;
+      const int d = std::abs(static_cast<int>(p / Np) - e);
+      reach = std::max(reach, std::min(d, Ne - d));
+    }
+  // Smallest chunk: 512 elements, or 2^18 nodes (2 MB of FP64 state) where
+  // that is fewer.  The chunk the last upload lands in and its neighbours
+  // to a depth of three (one per stage) finish after it, so the three first
+  // and four last chunks are thin: one reach each.
+  const int min_chunk = std::max(1, std::min(512, (1 << 18) / h->Np));
+  const int thin = std::max(min_chunk, reach);
+  std::vector<int> e0;
+  if (Ne < 9 * thin) {
+    const int S = std::min(16, Ne / min_chunk);
+    if (S < 4) return SDG_OK;
+    for (int j = 0; j <= S; ++j) e0.push_back(static_cast<int>(static_cast<long>(Ne) * j / S));
+  } else {
+    const int mid = Ne - 7 * thin;
+    const int target = std::max(min_chunk, Ne / 16);
+    const int M = std::max(1, (mid + target / 2) / target);
+    for (int j = 0; j <= 3; ++j) e0.push_back(j * thin);
+    for (int j = 1; j <= M; ++j)
+      e0.push_back(3 * thin + static_cast<int>(static_cast<long>(mid) * j / M));
+    for (int j = 1; j <= 4; ++j) e0.push_back(3 * thin + mid + j * thin);
+  }
+  const int S = static_cast<int>(e0.size()) - 1;
   auto chunk_of = [&](int e) {
     return static_cast<int>(std::upper_bound(e0.begin(), e0.end(), e) - e0.begin()) - 1;
   };
@@ -588,12 +652,8 @@ int build_chunks(sdg_handle* h) {
   // the other way round (the relation is made symmetric, so that every
   // chunk that reads a chunk's stage input in stage g precedes that chunk's
   // stage g + 2, which overwrites its q0 in stage 3).
-  auto neighbours = [&](const int* dpb, bool halo_ok, std::vector<std::vector<int>>* nbr,
-                        std::vector<char>* halo) -> bool {
-    std::vector<int> pb(6 * static_cast<size_t>(h->Ne));
-    if (cudaMemcpy(pb.data(), dpb, pb.size() * sizeof(int), cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
-      return false;
+  auto neighbours = [&](const std::vector<int>& pb, bool halo_ok,
+                        std::vector<std::vector<int>>* nbr, std::vector<char>* halo) -> bool {
     std::vector<std::vector<char>> hit(S, std::vector<char>(S, 0));
     halo->assign(S, 0);
     for (int j = 0; j < S; ++j) {
@@ -606,7 +666,7 @@ int build_chunks(sdg_handle* h) {
             (*halo)[j] = 1;
             continue;
           }
-          const int c = chunk_of(p / h->Np);
+          const int c = chunk_of(static_cast<int>(p / Np));
           hit[j][c] = hit[c][j] = 1;
         }
     }
@@ -618,9 +678,8 @@ int build_chunks(sdg_handle* h) {
   };
   std::vector<std::vector<int>> nbr, nbr_h;
   std::vector<char> unused, halo;
-  if (!neighbours(h->pb_halo, true, &nbr_h, &halo))
-    return fail(SDG_ERR_CUDA, "reading the face-neighbour table failed");
-  if (!h->direct_ok || !neighbours(h->pb_direct, false, &nbr, &unused)) nbr.clear();
+  neighbours(pbh, true, &nbr_h, &halo);
+  if (!h->direct_ok || !neighbours(pbd, false, &nbr, &unused)) nbr.clear();
   if (!h->copy_in) {
     SDG_CUDA(cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking));
     SDG_CUDA(cudaStreamCreateWithFlags(&h->copy_out, cudaStreamNonBlocking));
@@ -757,16 +816,28 @@ int enqueue_step_chunked(sdg_handle* h, double dt, bool uploads, double* host) {
       ++avail;
       continue;
     }
+    // The chunks after bj that are ready for the same stage join its launch
+    // (the step's last chunks, whose stages all wait for the last upload).
+    int bl = bj;
+    while (bl + 1 < S && !done[bg * S + bl + 1]) {
+      bool ok = true;
+      for (int c : h->chunk_nbr[bl + 1])
+        ok = ok && (bg == 0 ? c <= avail : done[(bg - 1) * S + c] != 0);
+      if (!ok) break;
+      ++bl;
+      if (bg == 0)
+        for (int c : h->chunk_nbr[bl]) need = std::max(need, c);
+    }
     if (bg == 0 && uploads && need > waited) {
       SDG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_up[need], 0));
       waited = need;
     }
-    const int e0 = h->chunk_e0[bj], n = h->chunk_e0[bj + 1] - e0;
+    const int e0 = h->chunk_e0[bj], n = h->chunk_e0[bl + 1] - e0;
     int rc = enqueue_stage_range(h, bg, dt, e0, n);
     if (rc) return rc;
     ++h->launches;
-    done[bg * S + bj] = 1;
-    --left;
+    for (int j = bj; j <= bl; ++j) done[bg * S + j] = 1;
+    left -= bl - bj + 1;
     if (bg == 2 && host) {
       SDG_CUDA(cudaEventRecord(h->ev_fin[bj], h->stream));
       SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_fin[bj], 0));
@@ -775,6 +846,83 @@ int enqueue_step_chunked(sdg_handle* h, double dt, bool uploads, double* host) {
     }
   }
   return SDG_OK;
+}
+
+// Enqueues nsteps >= 1 RK3 steps of sdg_rk3_steps_host: the chunk uploads
+// of q on copy_in, the first and last steps by chunks (the ones between
+// through the step graph), the chunk downloads into q on copy_out, and the
+// join of both copy streams into the handle's stream, so that later work
+// there (which may overwrite q0) follows the download.
+int enqueue_host_steps(sdg_handle* h, double* q, double dt, int nsteps) {
+  const int S = static_cast<int>(h->chunk_e0.size()) - 1;
+  const size_t Np = static_cast<size_t>(h->Np);
+  // The uploads overwrite q0: after everything already on the stream.
+  SDG_CUDA(cudaEventRecord(h->ev_in, h->stream));
+  SDG_CUDA(cudaStreamWaitEvent(h->copy_in, h->ev_in, 0));
+  SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_in, 0));
+  for (int j = 0; j < S; ++j) {
+    const int e0 = h->chunk_e0[j], n = h->chunk_e0[j + 1] - e0;
+    SDG_CUDA(cudaMemcpyAsync(h->q0 + e0 * Np, q + e0 * Np, n * Np * sizeof(double),
+                             cudaMemcpyHostToDevice, h->copy_in));
+    SDG_CUDA(cudaEventRecord(h->ev_up[j], h->copy_in));
+  }
+  int rc = enqueue_step_chunked(h, dt, true, nsteps == 1 ? q : nullptr);
+  if (!rc && nsteps > 1) {
+    for (int i = 0; i < nsteps - 2 && !rc; ++i)
+      if (cudaGraphLaunch(h->graph, h->stream) != cudaSuccess)
+        rc = fail(SDG_ERR_CUDA, "graph launch failed");
+    h->launches += 3LL * std::max(0, nsteps - 2);
+    if (!rc) rc = enqueue_step_chunked(h, dt, false, q);
+  }
+  cudaEventRecord(h->ev_out, h->copy_out);
+  cudaStreamWaitEvent(h->stream, h->ev_out, 0);
+  cudaEventRecord(h->ev_in, h->copy_in);
+  cudaStreamWaitEvent(h->stream, h->ev_in, 0);
+  return rc;
+}
+
+// One step of sdg_rk3_steps_host from pinned host array q as a CUDA graph
+// (captured on first use for q and dt): one submission instead of ~60
+// launches, copies and event operations.  While the copies run, a chunk's
+// stage kernel takes about twice its time alone (FP64 32^3 p = 7: median
+// 44 against 21 us, with ~26 against 3 us between launches); the graph
+// takes back little of that (one step 3.95 against 3.99 ms).
+int ensure_host_graph(sdg_handle* h, double* q, double dt) {
+  if (h->host_graph && h->host_graph_q == q && h->host_graph_dt == dt) return SDG_OK;
+  if (h->host_graph) cudaGraphExecDestroy(h->host_graph);
+  h->host_graph = nullptr;
+  h->host_graph_q = nullptr;
+  const long long l0 = h->launches;
+  cudaGraph_t g;
+  SDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_host_steps(h, q, dt, 1);
+  cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
+  h->host_graph_launches = h->launches - l0;
+  h->launches = l0;
+  if (ee == cudaSuccess && rc) cudaGraphDestroy(g);
+  if (rc) return rc;
+  if (ee != cudaSuccess)
+    return fail(SDG_ERR_CUDA, "host-step graph capture failed: %s", cudaGetErrorString(ee));
+  ee = cudaGraphInstantiate(&h->host_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ee != cudaSuccess) {
+    h->host_graph = nullptr;
+    return fail(SDG_ERR_CUDA, "host-step graph instantiate failed: %s",
+                cudaGetErrorString(ee));
+  }
+  h->host_graph_q = q;
+  h->host_graph_dt = dt;
+  return SDG_OK;
+}
+
+// Page-locked (or registered) host memory, which a captured copy needs.
+bool pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
 }
 
 }  // namespace
@@ -1055,35 +1203,19 @@ int sdg_rk3_steps_host(sdg_handle* h, double* q, double dt, int nsteps) {
   if ((rc = prime_stages(h))) return rc;
   if (nsteps > 2 && (rc = ensure_graph(h, dt))) return rc;
   account_rk(h);
-  const int S = static_cast<int>(h->chunk_e0.size()) - 1;
-  const size_t Np = static_cast<size_t>(h->Np);
-  // The uploads overwrite q0: after everything already on the stream.
-  SDG_CUDA(cudaEventRecord(h->ev_in, h->stream));
-  SDG_CUDA(cudaStreamWaitEvent(h->copy_in, h->ev_in, 0));
-  SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_in, 0));
-  for (int j = 0; j < S; ++j) {
-    const int e0 = h->chunk_e0[j], n = h->chunk_e0[j + 1] - e0;
-    SDG_CUDA(cudaMemcpyAsync(h->q0 + e0 * Np, q + e0 * Np, n * Np * sizeof(double),
-                             cudaMemcpyHostToDevice, h->copy_in));
-    SDG_CUDA(cudaEventRecord(h->ev_up[j], h->copy_in));
-  }
   h->have_q = true;
-  rc = enqueue_step_chunked(h, dt, true, nsteps == 1 ? q : nullptr);
-  if (!rc && nsteps > 1) {
-    for (int i = 0; i < nsteps - 2 && !rc; ++i)
-      if (cudaGraphLaunch(h->graph, h->stream) != cudaSuccess)
-        rc = fail(SDG_ERR_CUDA, "graph launch failed");
-    h->launches += 3LL * std::max(0, nsteps - 2);
-    if (!rc) rc = enqueue_step_chunked(h, dt, false, q);
+  const size_t NE = static_cast<size_t>(h->Np) * h->Ne;
+  if (nsteps == 1 && pinned(q) && pinned(q + NE - 1)) {
+    if ((rc = ensure_host_graph(h, q, dt))) return rc;
+    SDG_CUDA(cudaGraphLaunch(h->host_graph, h->stream));
+    h->launches += h->host_graph_launches;
+  } else if ((rc = enqueue_host_steps(h, q, dt, nsteps))) {
+    cudaStreamSynchronize(h->stream);
+    return rc;
   }
-  // Later work on the stream (which may overwrite q0) follows the download.
-  cudaEventRecord(h->ev_out, h->copy_out);
-  cudaStreamWaitEvent(h->stream, h->ev_out, 0);
-  cudaError_t e = cudaStreamSynchronize(h->copy_out);
-  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess)
     return fail(SDG_ERR_CUDA, "sdg_rk3_steps_host: %s", cudaGetErrorString(e));
-  SDG_CUDA(cudaStreamSynchronize(h->stream));
   return check_status(h);
 }
 
@@ -1204,10 +1336,7 @@ int sdg_set_kernel_variant(sdg_handle* h, int variant) {
     return fail(SDG_ERR_ARG, "kernel variant must be 0 (auto), 1 (block), 2 (pipelined), "
                 "3 (block, 8 blocks per SM), 4 (pipelined, split columns) or 5 "
                 "(pipelined, tensor-core lines of the mixed form at p = 7)");
-  if (variant != h->variant && h->graph) {
-    cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
-  }
+  if (variant != h->variant) drop_graphs(h);
   h->variant = variant;
   h->primed = false;
   return SDG_OK;
@@ -1218,10 +1347,7 @@ int sdg_debug_inject_wait_timeout(sdg_handle* h, int tile, int spins) {
   if (spins < 0) return fail(SDG_ERR_ARG, "spins must be >= 0");
   cudaSetDevice(h->dev);
   cudaStreamSynchronize(h->stream);
-  if (h->graph) {  // the step graph holds the old kernel arguments
-    cudaGraphExecDestroy(h->graph);
-    h->graph = nullptr;
-  }
+  drop_graphs(h);  // the graphs hold the old kernel arguments
   h->inject_skip = tile >= 0 ? tile + 1 : 0;
   h->wait_spins = static_cast<unsigned>(spins);
   return SDG_OK;

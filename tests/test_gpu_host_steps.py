@@ -58,6 +58,9 @@ def pinned_copy(q, mesh):
     ((12, 12, 16), 7, 0, 1),                    # DMMA lines, two elements a tile
     ((8, 8, 32), 9, 0, 1),                      # split-column kernel
     ((4, 4, 4), 3, 0, 2),                       # too small: the three calls
+    ((16, 16, 32), 3, 0, 2),                    # thin end chunks, 16 chunks
+    ((16, 16, 32), 2, sdg.FLAG_EXACT, 1),       # the same, exact arithmetic
+    ((8, 8, 16), 15, sdg.FLAG_MIXED, 1),        # thin chunks of one z-layer
 ])
 def test_host_steps_equal_three_calls(dims, p, flags, nsteps):
     ops, mesh, fields, dt = make(dims, p, flags)
@@ -112,6 +115,7 @@ def test_host_steps_argument_errors():
 
 @pytest.mark.parametrize("dims,p,flags", [
     ((16, 16, 8), 1, sdg.FLAG_EXACT),
+    ((16, 16, 32), 3, 0),
     ((13, 16, 20), 2, 0),
     ((12, 12, 16), 7, 0),
 ])
