@@ -137,3 +137,39 @@ def test_chunked_tendency_call_equals_device_call(dims, p, flags):
     ref = out.cpu().numpy().reshape(mesh.Np, mesh.NeA, order="F")[:, : mesh.Ne]
     h.close()
     assert np.array_equal(got, ref)
+
+
+def test_host_step_graph_follows_array_dt_and_hooks():
+    """A one-step call on pinned memory replays a CUDA graph captured for
+    that host array and dt: another array, another dt and the wait-timeout
+    test hook (whose kernel arguments the graph holds) each take a new
+    capture, and every result still equals the three calls."""
+    ops, mesh, fields, dt = make((16, 16, 16), 3, 0)
+    h = sdg.Handle(ops, mesh, 0)
+    h.set_kernel_variant(sdg.VARIANT_PIPE)   # the kernel the hook acts in
+    for which, a in zip((sdg.FIELD_U, sdg.FIELD_V, sdg.FIELD_W), fields[1:]):
+        h.set_field(which, a)
+    _ka, a = pinned_copy(fields[0], mesh)
+    _kb, b = pinned_copy(fields[0], mesh)
+    h.rk3_steps_host(a, dt, 1)
+    h.rk3_steps_host(b, dt, 1)           # another array
+    h.rk3_steps_host(a, 0.5 * dt, 1)     # another dt
+    h.rk3_steps_host(b, dt, 1)
+    one = three_calls(ops, mesh, 0, fields, dt, 1)
+    rest = tuple(fields[1:])
+    want_a = three_calls(ops, mesh, 0, (one,) + rest, 0.5 * dt, 1)
+    want_b = three_calls(ops, mesh, 0, (one,) + rest, dt, 1)
+    assert np.array_equal(a.reshape(mesh.Np, mesh.Ne, order="F"), want_a)
+    assert np.array_equal(b.reshape(mesh.Np, mesh.Ne, order="F"), want_b)
+    # The same array and dt again, now with the hook on: a replay of the
+    # old graph would not see it.
+    h.inject_wait_timeout(0, spins=1024)
+    with pytest.raises(sdg.SdgError) as ei:
+        h.rk3_steps_host(a, 0.5 * dt, 1)
+    assert ei.value.code == sdg.SDG_ERR_CUDA
+    assert "timed out" in str(ei.value)
+    h.inject_wait_timeout(-1)
+    a[:] = np.asarray(fields[0]).reshape(-1, order="F")[: mesh.Np * mesh.Ne]
+    h.rk3_steps_host(a, dt, 1)
+    h.close()
+    assert np.array_equal(a.reshape(mesh.Np, mesh.Ne, order="F"), one)
