@@ -273,6 +273,20 @@ int sdg_set_kernel_variant(sdg_handle* h, int variant);
  * usable throughout.  Only the pipelined kernel variant has waits. */
 int sdg_debug_inject_wait_timeout(sdg_handle* h, int tile, int spins);
 
+/* Host logic of sdg_rk3_steps_host and the chunked sdg_cal_tend, exposed
+ * for tests (no device needed).  sdg_debug_chunk_bounds: the chunk
+ * boundaries e0[0..S] (S + 1 values, at most cap) that Ne elements of Np
+ * nodes get when face neighbours lie within cyclic index distance `reach`
+ * (NeX * NeY in a periodic box); *nchunks = S, 0 when the mesh is too small
+ * to pipeline.  sdg_debug_step_plan: the launches of one chunked RK step
+ * over S chunks whose neighbour lists (each holding the chunk itself;
+ * symmetric) are nbr_idx[nbr_ptr[j] .. nbr_ptr[j+1]-1], with or without the
+ * chunk uploads: *nops launches as (stage 0..2, first chunk, last chunk,
+ * upload to wait for or -1) in ops[4 * nops], at most cap ints. */
+int sdg_debug_chunk_bounds(int Ne, int Np, int reach, int* e0, int cap, int* nchunks);
+int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int uploads, int* ops,
+                        int cap, int* nops);
+
 /* ---------------------------------------------------------------------
  * Batched ensembles: many independent periodic-box instances of uneven
  * size and order advanced together (the reference runs one mesh per

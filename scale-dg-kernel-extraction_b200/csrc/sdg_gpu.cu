@@ -578,6 +578,96 @@ void drop_graphs(sdg_handle* h) {
   h->host_graph_q = nullptr;
 }
 
+// Chunk boundaries e0[0..S] of Ne elements of Np nodes whose face
+// neighbours lie within cyclic index distance `reach` (empty: fewer than 4
+// chunks, no pipelining).  Smallest chunk: 512 elements, or 2^18 nodes
+// (2 MB of FP64 state) where that is fewer.  The chunk the last upload
+// lands in and its neighbours to a depth of three (one per stage) finish
+// after it, so the three first and four last chunks are thin, one reach
+// each, and the ones between them about Ne/16.
+std::vector<int> chunk_bounds(int Ne, int Np, int reach) {
+  const int min_chunk = std::max(1, std::min(512, (1 << 18) / Np));
+  const int thin = std::max(min_chunk, reach);
+  std::vector<int> e0;
+  if (Ne < 9 * thin) {
+    const int S = std::min(16, Ne / min_chunk);
+    if (S < 4) return e0;
+    for (int j = 0; j <= S; ++j) e0.push_back(static_cast<int>(static_cast<long>(Ne) * j / S));
+  } else {
+    const int mid = Ne - 7 * thin;
+    const int target = std::max(min_chunk, Ne / 16);
+    const int M = std::max(1, (mid + target / 2) / target);
+    for (int j = 0; j <= 3; ++j) e0.push_back(j * thin);
+    for (int j = 1; j <= M; ++j)
+      e0.push_back(3 * thin + static_cast<int>(static_cast<long>(mid) * j / M));
+    for (int j = 1; j <= 4; ++j) e0.push_back(3 * thin + mid + j * thin);
+  }
+  return e0;
+}
+
+// One launch of a chunked RK step: stage g (0..2) over chunks j0..j1, after
+// the upload of chunk `need` (stage 0 with uploads; -1: no upload to wait
+// for).
+struct StepOp {
+  int g, j0, j1, need;
+};
+
+// The launches of one chunked RK step, in enqueue order.  Stage g of chunk
+// j needs stage g-1 of every chunk in nbr[j] (which holds j and is
+// symmetric); stage 0 needs those chunks uploaded, in chunk order, when
+// `uploads` is set.  Ready work goes first, the latest stage first, so that
+// chunks finish (and go back) early.  With uploads, the chunks after the
+// first ready one that are ready for the same stage join its launch: the
+// step's last chunks, whose stages all wait for the last upload.  Empty when
+// the lists admit no schedule (a neighbour index outside 0..S-1).
+std::vector<StepOp> plan_step(int S, const std::vector<std::vector<int>>& nbr, bool uploads) {
+  std::vector<StepOp> ops;
+  std::vector<char> done(3 * static_cast<size_t>(S), 0);
+  for (const auto& l : nbr)
+    for (int c : l)
+      if (c < 0 || c >= S) return ops;
+  auto ready = [&](int g, int j, int avail, int* need) {
+    for (int c : nbr[j]) {
+      if (g == 0) {
+        *need = std::max(*need, c);
+        if (c > avail) return false;
+      } else if (!done[(g - 1) * S + c]) {
+        return false;
+      }
+    }
+    return true;
+  };
+  int avail = uploads ? -1 : S - 1;  // uploads the stream may rely on
+  int left = 3 * S;
+  while (left > 0) {
+    int bg = -1, bj = -1, need = -1;
+    for (int g = 2; g >= 0 && bg < 0; --g)
+      for (int j = 0; j < S && bg < 0; ++j) {
+        int nu = -1;
+        if (!done[g * S + j] && ready(g, j, avail, &nu)) {
+          bg = g;
+          bj = j;
+          need = nu;
+        }
+      }
+    if (bg < 0) {  // nothing ready: rely on the next upload
+      if (++avail >= S) return {};
+      continue;
+    }
+    int bl = bj;
+    while (uploads && bl + 1 < S && !done[bg * S + bl + 1]) {
+      int nu = need;
+      if (!ready(bg, bl + 1, avail, &nu)) break;
+      need = nu;
+      ++bl;
+    }
+    ops.push_back({bg, bj, bl, bg == 0 && uploads ? need : -1});
+    for (int j = bj; j <= bl; ++j) done[bg * S + j] = 1;
+    left -= bl - bj + 1;
+  }
+  return ops;
+}
+
 // Element chunks of sdg_rk3_steps_host and sdg_cal_tend: S contiguous
 // element ranges (fewer than 4 chunks do not pipeline) and, per chunk, the
 // chunks that hold a face neighbour of one of its elements, through the
@@ -624,26 +714,8 @@ int build_chunks(sdg_handle* h) {
       const int d = std::abs(static_cast<int>(p / Np) - e);
       reach = std::max(reach, std::min(d, Ne - d));
     }
-  // Smallest chunk: 512 elements, or 2^18 nodes (2 MB of FP64 state) where
-  // that is fewer.  The chunk the last upload lands in and its neighbours
-  // to a depth of three (one per stage) finish after it, so the three first
-  // and four last chunks are thin: one reach each.
-  const int min_chunk = std::max(1, std::min(512, (1 << 18) / h->Np));
-  const int thin = std::max(min_chunk, reach);
-  std::vector<int> e0;
-  if (Ne < 9 * thin) {
-    const int S = std::min(16, Ne / min_chunk);
-    if (S < 4) return SDG_OK;
-    for (int j = 0; j <= S; ++j) e0.push_back(static_cast<int>(static_cast<long>(Ne) * j / S));
-  } else {
-    const int mid = Ne - 7 * thin;
-    const int target = std::max(min_chunk, Ne / 16);
-    const int M = std::max(1, (mid + target / 2) / target);
-    for (int j = 0; j <= 3; ++j) e0.push_back(j * thin);
-    for (int j = 1; j <= M; ++j)
-      e0.push_back(3 * thin + static_cast<int>(static_cast<long>(mid) * j / M));
-    for (int j = 1; j <= 4; ++j) e0.push_back(3 * thin + mid + j * thin);
-  }
+  const std::vector<int> e0 = chunk_bounds(Ne, h->Np, reach);
+  if (e0.empty()) return SDG_OK;
   const int S = static_cast<int>(e0.size()) - 1;
   auto chunk_of = [&](int e) {
     return static_cast<int>(std::upper_bound(e0.begin(), e0.end(), e) - e0.begin()) - 1;
@@ -778,69 +850,27 @@ int cal_tend_chunked(sdg_handle* h, double* dqdt, const double* const src[4]) {
 }
 
 // Enqueues the three stages of one RK3 step chunk by chunk on the handle's
-// stream.  Stage g of chunk j needs stage g-1 of every neighbour chunk (the
-// step's input for g = 0: with `uploads`, the chunks' host-to-device copies
-// on copy_in, in chunk order, each followed by its ev_up event).  Ready work
-// goes first, the latest stage first, so chunks finish early; with
-// `downloads`, each chunk's final state is copied to host[] on copy_out
-// once its stage 3 is done.
+// stream, in the order of plan_step; stage-1 launches wait for the uploads
+// they need (ev_up events of copy_in).  With `host`, each chunk's final
+// state is copied to host[] on copy_out once its stage 3 is done.
 int enqueue_step_chunked(sdg_handle* h, double dt, bool uploads, double* host) {
   const int S = static_cast<int>(h->chunk_e0.size()) - 1;
   const size_t Np = static_cast<size_t>(h->Np);
-  std::vector<char> done(3 * static_cast<size_t>(S), 0);
-  int avail = uploads ? -1 : S - 1;  // uploads the stream may rely on
-  int waited = -1;                   // uploads it already waits for
-  int left = 3 * S;
-  while (left > 0) {
-    int bg = -1, bj = -1, need = -1;
-    for (int g = 2; g >= 0 && bg < 0; --g)
-      for (int j = 0; j < S && bg < 0; ++j) {
-        if (done[g * S + j]) continue;
-        bool ok = true;
-        int nu = -1;
-        for (int c : h->chunk_nbr[j]) {
-          if (g == 0) {
-            nu = std::max(nu, c);
-            ok = ok && c <= avail;
-          } else {
-            ok = ok && done[(g - 1) * S + c];
-          }
-        }
-        if (ok) {
-          bg = g;
-          bj = j;
-          need = nu;
-        }
-      }
-    if (bg < 0) {  // nothing ready: rely on the next upload
-      ++avail;
-      continue;
+  const std::vector<StepOp> ops = plan_step(S, h->chunk_nbr, uploads);
+  if (ops.empty()) return fail(SDG_ERR_STATE, "no schedule for the element chunks");
+  int waited = -1;  // uploads the stream already waits for
+  for (const StepOp& op : ops) {
+    if (op.need > waited) {
+      SDG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_up[op.need], 0));
+      waited = op.need;
     }
-    // The chunks after bj that are ready for the same stage join its launch
-    // (the step's last chunks, whose stages all wait for the last upload).
-    int bl = bj;
-    while (bl + 1 < S && !done[bg * S + bl + 1]) {
-      bool ok = true;
-      for (int c : h->chunk_nbr[bl + 1])
-        ok = ok && (bg == 0 ? c <= avail : done[(bg - 1) * S + c] != 0);
-      if (!ok) break;
-      ++bl;
-      if (bg == 0)
-        for (int c : h->chunk_nbr[bl]) need = std::max(need, c);
-    }
-    if (bg == 0 && uploads && need > waited) {
-      SDG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_up[need], 0));
-      waited = need;
-    }
-    const int e0 = h->chunk_e0[bj], n = h->chunk_e0[bl + 1] - e0;
-    int rc = enqueue_stage_range(h, bg, dt, e0, n);
+    const int e0 = h->chunk_e0[op.j0], n = h->chunk_e0[op.j1 + 1] - e0;
+    int rc = enqueue_stage_range(h, op.g, dt, e0, n);
     if (rc) return rc;
     ++h->launches;
-    for (int j = bj; j <= bl; ++j) done[bg * S + j] = 1;
-    left -= bl - bj + 1;
-    if (bg == 2 && host) {
-      SDG_CUDA(cudaEventRecord(h->ev_fin[bj], h->stream));
-      SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_fin[bj], 0));
+    if (op.g == 2 && host) {
+      SDG_CUDA(cudaEventRecord(h->ev_fin[op.j0], h->stream));
+      SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_fin[op.j0], 0));
       SDG_CUDA(cudaMemcpyAsync(host + e0 * Np, h->q0 + e0 * Np, n * Np * sizeof(double),
                                cudaMemcpyDeviceToHost, h->copy_out));
     }
@@ -1339,6 +1369,42 @@ int sdg_set_kernel_variant(sdg_handle* h, int variant) {
   if (variant != h->variant) drop_graphs(h);
   h->variant = variant;
   h->primed = false;
+  return SDG_OK;
+}
+
+int sdg_debug_chunk_bounds(int Ne, int Np, int reach, int* e0, int cap, int* nchunks) {
+  if (Ne < 1 || Np < 1 || reach < 1 || !nchunks || cap < 0 || (cap > 0 && !e0))
+    return fail(SDG_ERR_ARG, "sdg_debug_chunk_bounds: bad argument");
+  const std::vector<int> b = chunk_bounds(Ne, Np, reach);
+  *nchunks = b.empty() ? 0 : static_cast<int>(b.size()) - 1;
+  if (static_cast<int>(b.size()) > cap)
+    return fail(SDG_ERR_ARG, "sdg_debug_chunk_bounds: %d boundaries, room for %d",
+                static_cast<int>(b.size()), cap);
+  std::copy(b.begin(), b.end(), e0);
+  return SDG_OK;
+}
+
+int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int uploads, int* ops,
+                        int cap, int* nops) {
+  if (S < 1 || !nbr_ptr || !nbr_idx || !nops || cap < 0 || (cap > 0 && !ops))
+    return fail(SDG_ERR_ARG, "sdg_debug_step_plan: bad argument");
+  std::vector<std::vector<int>> nbr(S);
+  for (int j = 0; j < S; ++j) {
+    if (nbr_ptr[j + 1] < nbr_ptr[j])
+      return fail(SDG_ERR_ARG, "sdg_debug_step_plan: nbr_ptr decreases at %d", j);
+    nbr[j].assign(nbr_idx + nbr_ptr[j], nbr_idx + nbr_ptr[j + 1]);
+  }
+  const std::vector<StepOp> p = plan_step(S, nbr, uploads != 0);
+  if (p.empty()) return fail(SDG_ERR_ARG, "sdg_debug_step_plan: the lists admit no schedule");
+  *nops = static_cast<int>(p.size());
+  if (4 * *nops > cap)
+    return fail(SDG_ERR_ARG, "sdg_debug_step_plan: %d launches, room for %d", *nops, cap / 4);
+  for (size_t i = 0; i < p.size(); ++i) {
+    ops[4 * i] = p[i].g;
+    ops[4 * i + 1] = p[i].j0;
+    ops[4 * i + 2] = p[i].j1;
+    ops[4 * i + 3] = p[i].need;
+  }
   return SDG_OK;
 }
 

@@ -85,6 +85,8 @@ SIGNATURES = {
     "sdg_launch_count": (_LL, [_P]),
     "sdg_set_kernel_variant": (_I, [_P, _I]),
     "sdg_debug_inject_wait_timeout": (_I, [_P, _I, _I]),
+    "sdg_debug_chunk_bounds": (_I, [_I, _I, _I, _P, _I, ctypes.POINTER(_I)]),
+    "sdg_debug_step_plan": (_I, [_I, _P, _P, _I, _P, _I, ctypes.POINTER(_I)]),
     "sdg_minmax_dev_noalloc": (_I, [_P, _LL, _P, _P]),
     "sdg_divlike_dev": (_I, [_I, _I, _LL, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "sdg_gradlike_dev": (_I, [_I, _LL, _P, _P, _P, _P, _P, _I, _P]),
@@ -412,6 +414,31 @@ class Handle:
         `tile`, so its bounded wait runs out after `spins` polls and the next
         synchronising call raises; tile < 0 turns it off."""
         _check(lib().sdg_debug_inject_wait_timeout(self._h, tile, spins))
+
+
+def chunk_bounds(Ne, Np, reach):
+    """Element-chunk boundaries of the host-buffer calls for Ne elements of
+    Np nodes whose face neighbours lie within cyclic index distance `reach`
+    (host logic, no device needed); empty when the mesh does not pipeline."""
+    e0 = np.zeros(64, dtype=np.int32)
+    n = ctypes.c_int(0)
+    _check(lib().sdg_debug_chunk_bounds(Ne, Np, reach, _p(e0), e0.size, ctypes.byref(n)))
+    return e0[: n.value + 1] if n.value else e0[:0]
+
+
+def step_plan(nbr, uploads):
+    """Launch order of one chunked RK step over len(nbr) chunks with
+    neighbour lists nbr (host logic): rows (stage, first chunk, last chunk,
+    upload waited for or -1)."""
+    S = len(nbr)
+    ptr = np.zeros(S + 1, dtype=np.int32)
+    ptr[1:] = np.cumsum([len(l) for l in nbr])
+    idx = np.array([c for l in nbr for c in l] or [0], dtype=np.int32)
+    ops = np.zeros(4 * 3 * S, dtype=np.int32)
+    n = ctypes.c_int(0)
+    _check(lib().sdg_debug_step_plan(S, _p(ptr), _p(idx), int(bool(uploads)), _p(ops),
+                                     ops.size, ctypes.byref(n)))
+    return ops[: 4 * n.value].reshape(-1, 4)
 
 
 def _device_view(ptr, n, dtype):
