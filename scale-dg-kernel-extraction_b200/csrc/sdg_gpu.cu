@@ -558,6 +558,7 @@ int ensure_graph(sdg_handle* h, double dt) {
   SDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int rc = enqueue_step(h, dt);
   cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
+  if (ee == cudaSuccess && rc) cudaGraphDestroy(g);
   if (rc) return rc;
   if (ee != cudaSuccess)
     return fail(SDG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ee));
