@@ -1374,7 +1374,7 @@ int sdg_set_kernel_variant(sdg_handle* h, int variant) {
 }
 
 int sdg_debug_chunk_bounds(int Ne, int Np, int reach, int* e0, int cap, int* nchunks) {
-  if (Ne < 1 || Np < 1 || reach < 1 || !nchunks || cap < 0 || (cap > 0 && !e0))
+  if (Ne < 1 || Np < 1 || reach < 1 || reach > Ne || !nchunks || cap < 0 || (cap > 0 && !e0))
     return fail(SDG_ERR_ARG, "sdg_debug_chunk_bounds: bad argument");
   const std::vector<int> b = chunk_bounds(Ne, Np, reach);
   *nchunks = b.empty() ? 0 : static_cast<int>(b.size()) - 1;

@@ -124,3 +124,10 @@ def test_step_plan_rejects_bad_lists():
     with pytest.raises(sdg.SdgError) as e:
         sdg.step_plan([[0, 1], [0, 5]], uploads=True)
     assert e.value.code == sdg.SDG_ERR_ARG
+
+
+def test_chunk_bounds_rejects_bad_arguments():
+    for args in ((0, 64, 1), (64, 0, 1), (64, 64, 0), (64, 64, 65)):
+        with pytest.raises(sdg.SdgError) as e:
+            sdg.chunk_bounds(*args)
+        assert e.value.code == sdg.SDG_ERR_ARG
