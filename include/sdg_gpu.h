@@ -198,8 +198,11 @@ int sdg_rk3_steps(sdg_handle* h, double dt, int nsteps);
  * chunk as soon as the chunks they read are uploaded, the last step's as
  * the state's chunks go back, so the two copies and the stages overlap
  * (host memory pinned with cudaHostAlloc / cudaHostRegister for the copies
- * to run asynchronously; a one-step call on pinned memory replays a CUDA
- * graph captured for that array and dt).  Meshes of fewer than 2,048
+ * to run asynchronously).  Calls of up to three steps run as one chunked
+ * plan, so that the first chunks' results go back while the last chunks go
+ * up, and on pinned memory replay a CUDA graph captured for that array, dt
+ * and step count; longer calls run the first and last steps by chunks and
+ * the ones between through the step graph.  Meshes of fewer than 2,048
  * elements (fewer than 4 chunks of 512 elements or 2^18 nodes), or whose
  * boundary faces read the halo buffer, take the three calls in order.
  * Velocities must be set (sdg_set_field).  Synchronises the handle. */
@@ -278,14 +281,15 @@ int sdg_debug_inject_wait_timeout(sdg_handle* h, int tile, int spins);
  * boundaries e0[0..S] (S + 1 values, at most cap) that Ne elements of Np
  * nodes get when face neighbours lie within cyclic index distance `reach`
  * (NeX * NeY in a periodic box); *nchunks = S, 0 when the mesh is too small
- * to pipeline.  sdg_debug_step_plan: the launches of one chunked RK step
- * over S chunks whose neighbour lists (each holding the chunk itself;
- * symmetric) are nbr_idx[nbr_ptr[j] .. nbr_ptr[j+1]-1], with or without the
- * chunk uploads: *nops launches as (stage 0..2, first chunk, last chunk,
- * upload to wait for or -1) in ops[4 * nops], at most cap ints. */
+ * to pipeline.  sdg_debug_step_plan: the launches of `steps` (1..64)
+ * chunked RK steps over S chunks whose neighbour lists (each holding the
+ * chunk itself; symmetric) are nbr_idx[nbr_ptr[j] .. nbr_ptr[j+1]-1], with
+ * or without the chunk uploads: *nops launches as (stage 0 .. 3*steps-1,
+ * first chunk, last chunk, upload to wait for or -1) in ops[4 * nops], at
+ * most cap ints. */
 int sdg_debug_chunk_bounds(int Ne, int Np, int reach, int* e0, int cap, int* nchunks);
-int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int uploads, int* ops,
-                        int cap, int* nops);
+int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int steps, int uploads,
+                        int* ops, int cap, int* nops);
 
 /* ---------------------------------------------------------------------
  * Batched ensembles: many independent periodic-box instances of uneven

@@ -234,12 +234,13 @@ struct sdg_handle {
   // Step graph.
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0.0;
-  // Graph of one sdg_rk3_steps_host step (uploads, chunked stages and
-  // downloads) for the pinned host array host_graph_q and host_graph_dt,
-  // and the number of kernels it launches.
+  // Graph of an sdg_rk3_steps_host call of host_graph_steps steps (uploads,
+  // chunked stages and downloads) for the pinned host array host_graph_q
+  // and host_graph_dt, and the number of kernels it launches.
   cudaGraphExec_t host_graph = nullptr;
   const double* host_graph_q = nullptr;
   double host_graph_dt = 0.0;
+  int host_graph_steps = 0;
   long long host_graph_launches = 0;
 
   // sdg_rk3_steps_host and sdg_cal_tend (lazy): element chunks (boundaries,
@@ -606,24 +607,39 @@ std::vector<int> chunk_bounds(int Ne, int Np, int reach) {
   return e0;
 }
 
-// One launch of a chunked RK step: stage g (0..2) over chunks j0..j1, after
-// the upload of chunk `need` (stage 0 with uploads; -1: no upload to wait
-// for).
+// One launch of chunked RK steps: stage g (0 .. 3 * steps - 1; RK stage
+// g % 3 of step g / 3) over chunks j0..j1, after the upload of chunk `need`
+// (stage 0 with uploads; -1: no upload to wait for).
 struct StepOp {
   int g, j0, j1, need;
 };
 
-// The launches of one chunked RK step, in enqueue order.  Stage g of chunk
-// j needs stage g-1 of every chunk in nbr[j] (which holds j and is
+// The launches of `steps` chunked RK steps, in enqueue order.  Stage g of
+// chunk j needs stage g-1 of every chunk in nbr[j] (which holds j and is
 // symmetric); stage 0 needs those chunks uploaded, in chunk order, when
-// `uploads` is set.  Ready work goes first, the latest stage first, so that
-// chunks finish (and go back) early.  With uploads, the chunks after the
-// first ready one that are ready for the same stage join its launch: the
-// step's last chunks, whose stages all wait for the last upload.  Empty when
-// the lists admit no schedule (a neighbour index outside 0..S-1).
-std::vector<StepOp> plan_step(int S, const std::vector<std::vector<int>>& nbr, bool uploads) {
+// `uploads` is set.  Stage g + 3 overwrites stage g's output buffer (and
+// the last stage of a step q0, which stage 0 of that step reads from the
+// neighbour chunks); it follows stage g + 2 of the neighbour chunks and so,
+// through them, every stage g + 1 that reads it.  Ready work goes first,
+// the latest stage first, so that chunks finish (and go back) early.  With
+// uploads, the chunks after the first ready one that are ready for the
+// same stage join its launch: the last chunks, whose stages all wait for
+// the last upload.  Empty when the lists admit no schedule (a neighbour
+// index outside 0..S-1).
+std::vector<StepOp> plan_steps(int S, const std::vector<std::vector<int>>& nbr, int steps,
+                               bool uploads);
+
+// sdg_rk3_steps_host plans up to this many steps as one: the final state of
+// a chunk then depends on the chunks within 3 * steps of it, so with more
+// steps nearly every chunk waits for the last upload and the plan buys no
+// overlap of the two copy directions.
+constexpr int kPlanSteps = 3;
+
+std::vector<StepOp> plan_steps(int S, const std::vector<std::vector<int>>& nbr, int steps,
+                               bool uploads) {
   std::vector<StepOp> ops;
-  std::vector<char> done(3 * static_cast<size_t>(S), 0);
+  const int G = 3 * steps;
+  std::vector<char> done(G * static_cast<size_t>(S), 0);
   for (const auto& l : nbr)
     for (int c : l)
       if (c < 0 || c >= S) return ops;
@@ -639,10 +655,10 @@ std::vector<StepOp> plan_step(int S, const std::vector<std::vector<int>>& nbr, b
     return true;
   };
   int avail = uploads ? -1 : S - 1;  // uploads the stream may rely on
-  int left = 3 * S;
+  int left = G * S;
   while (left > 0) {
     int bg = -1, bj = -1, need = -1;
-    for (int g = 2; g >= 0 && bg < 0; --g)
+    for (int g = G - 1; g >= 0 && bg < 0; --g)
       for (int j = 0; j < S && bg < 0; ++j) {
         int nu = -1;
         if (!done[g * S + j] && ready(g, j, avail, &nu)) {
@@ -850,14 +866,14 @@ int cal_tend_chunked(sdg_handle* h, double* dqdt, const double* const src[4]) {
   return rc;
 }
 
-// Enqueues the three stages of one RK3 step chunk by chunk on the handle's
-// stream, in the order of plan_step; stage-1 launches wait for the uploads
-// they need (ev_up events of copy_in).  With `host`, each chunk's final
-// state is copied to host[] on copy_out once its stage 3 is done.
-int enqueue_step_chunked(sdg_handle* h, double dt, bool uploads, double* host) {
+// Enqueues `steps` RK3 steps chunk by chunk on the handle's stream, in the
+// order of plan_steps; stage-1 launches wait for the uploads they need
+// (ev_up events of copy_in).  With `host`, each chunk's final state is
+// copied to host[] on copy_out once its last stage is done.
+int enqueue_steps_chunked(sdg_handle* h, double dt, int steps, bool uploads, double* host) {
   const int S = static_cast<int>(h->chunk_e0.size()) - 1;
   const size_t Np = static_cast<size_t>(h->Np);
-  const std::vector<StepOp> ops = plan_step(S, h->chunk_nbr, uploads);
+  const std::vector<StepOp> ops = plan_steps(S, h->chunk_nbr, steps, uploads);
   if (ops.empty()) return fail(SDG_ERR_STATE, "no schedule for the element chunks");
   int waited = -1;  // uploads the stream already waits for
   for (const StepOp& op : ops) {
@@ -866,10 +882,10 @@ int enqueue_step_chunked(sdg_handle* h, double dt, bool uploads, double* host) {
       waited = op.need;
     }
     const int e0 = h->chunk_e0[op.j0], n = h->chunk_e0[op.j1 + 1] - e0;
-    int rc = enqueue_stage_range(h, op.g, dt, e0, n);
+    int rc = enqueue_stage_range(h, op.g % 3, dt, e0, n);
     if (rc) return rc;
     ++h->launches;
-    if (op.g == 2 && host) {
+    if (op.g == 3 * steps - 1 && host) {
       SDG_CUDA(cudaEventRecord(h->ev_fin[op.j0], h->stream));
       SDG_CUDA(cudaStreamWaitEvent(h->copy_out, h->ev_fin[op.j0], 0));
       SDG_CUDA(cudaMemcpyAsync(host + e0 * Np, h->q0 + e0 * Np, n * Np * sizeof(double),
@@ -880,7 +896,8 @@ int enqueue_step_chunked(sdg_handle* h, double dt, bool uploads, double* host) {
 }
 
 // Enqueues nsteps >= 1 RK3 steps of sdg_rk3_steps_host: the chunk uploads
-// of q on copy_in, the first and last steps by chunks (the ones between
+// of q on copy_in, the steps by chunks (up to kPlanSteps of them as one
+// plan; beyond, the first and last steps by chunks and the ones between
 // through the step graph), the chunk downloads into q on copy_out, and the
 // join of both copy streams into the handle's stream, so that later work
 // there (which may overwrite q0) follows the download.
@@ -897,13 +914,19 @@ int enqueue_host_steps(sdg_handle* h, double* q, double dt, int nsteps) {
                              cudaMemcpyHostToDevice, h->copy_in));
     SDG_CUDA(cudaEventRecord(h->ev_up[j], h->copy_in));
   }
-  int rc = enqueue_step_chunked(h, dt, true, nsteps == 1 ? q : nullptr);
-  if (!rc && nsteps > 1) {
+  // Up to kPlanSteps steps as one plan, so that the last chunks' downloads
+  // overlap the uploads; beyond, the first and last steps by chunks and the
+  // ones between through the step graph.
+  int rc;
+  if (nsteps <= kPlanSteps) {
+    rc = enqueue_steps_chunked(h, dt, nsteps, true, q);
+  } else {
+    rc = enqueue_steps_chunked(h, dt, 1, true, nullptr);
     for (int i = 0; i < nsteps - 2 && !rc; ++i)
       if (cudaGraphLaunch(h->graph, h->stream) != cudaSuccess)
         rc = fail(SDG_ERR_CUDA, "graph launch failed");
-    h->launches += 3LL * std::max(0, nsteps - 2);
-    if (!rc) rc = enqueue_step_chunked(h, dt, false, q);
+    h->launches += 3LL * (nsteps - 2);
+    if (!rc) rc = enqueue_steps_chunked(h, dt, 1, false, q);
   }
   cudaEventRecord(h->ev_out, h->copy_out);
   cudaStreamWaitEvent(h->stream, h->ev_out, 0);
@@ -912,21 +935,23 @@ int enqueue_host_steps(sdg_handle* h, double* q, double dt, int nsteps) {
   return rc;
 }
 
-// One step of sdg_rk3_steps_host from pinned host array q as a CUDA graph
-// (captured on first use for q and dt): one submission instead of ~60
-// launches, copies and event operations.  While the copies run, a chunk's
+// An sdg_rk3_steps_host call of up to kPlanSteps steps from pinned host
+// array q as a CUDA graph (captured on first use for q, dt and nsteps): one
+// submission instead of ~60 launches, copies and event operations per step.  While the copies run, a chunk's
 // stage kernel takes about twice its time alone (FP64 32^3 p = 7: median
 // 44 against 21 us, with ~26 against 3 us between launches); the graph
 // takes back little of that (one step 3.95 against 3.99 ms).
-int ensure_host_graph(sdg_handle* h, double* q, double dt) {
-  if (h->host_graph && h->host_graph_q == q && h->host_graph_dt == dt) return SDG_OK;
+int ensure_host_graph(sdg_handle* h, double* q, double dt, int nsteps) {
+  if (h->host_graph && h->host_graph_q == q && h->host_graph_dt == dt &&
+      h->host_graph_steps == nsteps)
+    return SDG_OK;
   if (h->host_graph) cudaGraphExecDestroy(h->host_graph);
   h->host_graph = nullptr;
   h->host_graph_q = nullptr;
   const long long l0 = h->launches;
   cudaGraph_t g;
   SDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_host_steps(h, q, dt, 1);
+  int rc = enqueue_host_steps(h, q, dt, nsteps);
   cudaError_t ee = cudaStreamEndCapture(h->stream, &g);
   h->host_graph_launches = h->launches - l0;
   h->launches = l0;
@@ -943,6 +968,7 @@ int ensure_host_graph(sdg_handle* h, double* q, double dt) {
   }
   h->host_graph_q = q;
   h->host_graph_dt = dt;
+  h->host_graph_steps = nsteps;
   return SDG_OK;
 }
 
@@ -1232,12 +1258,12 @@ int sdg_rk3_steps_host(sdg_handle* h, double* q, double dt, int nsteps) {
     return sdg_get_field(h, SDG_FIELD_Q, q);
   }
   if ((rc = prime_stages(h))) return rc;
-  if (nsteps > 2 && (rc = ensure_graph(h, dt))) return rc;
+  if (nsteps > kPlanSteps && (rc = ensure_graph(h, dt))) return rc;
   account_rk(h);
   h->have_q = true;
   const size_t NE = static_cast<size_t>(h->Np) * h->Ne;
-  if (nsteps == 1 && pinned(q) && pinned(q + NE - 1)) {
-    if ((rc = ensure_host_graph(h, q, dt))) return rc;
+  if (nsteps <= kPlanSteps && pinned(q) && pinned(q + NE - 1)) {
+    if ((rc = ensure_host_graph(h, q, dt, nsteps))) return rc;
     SDG_CUDA(cudaGraphLaunch(h->host_graph, h->stream));
     h->launches += h->host_graph_launches;
   } else if ((rc = enqueue_host_steps(h, q, dt, nsteps))) {
@@ -1385,9 +1411,10 @@ int sdg_debug_chunk_bounds(int Ne, int Np, int reach, int* e0, int cap, int* nch
   return SDG_OK;
 }
 
-int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int uploads, int* ops,
-                        int cap, int* nops) {
-  if (S < 1 || !nbr_ptr || !nbr_idx || !nops || cap < 0 || (cap > 0 && !ops))
+int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int steps, int uploads,
+                        int* ops, int cap, int* nops) {
+  if (S < 1 || steps < 1 || steps > 64 || !nbr_ptr || !nbr_idx || !nops || cap < 0 ||
+      (cap > 0 && !ops))
     return fail(SDG_ERR_ARG, "sdg_debug_step_plan: bad argument");
   std::vector<std::vector<int>> nbr(S);
   for (int j = 0; j < S; ++j) {
@@ -1395,7 +1422,7 @@ int sdg_debug_step_plan(int S, const int* nbr_ptr, const int* nbr_idx, int uploa
       return fail(SDG_ERR_ARG, "sdg_debug_step_plan: nbr_ptr decreases at %d", j);
     nbr[j].assign(nbr_idx + nbr_ptr[j], nbr_idx + nbr_ptr[j + 1]);
   }
-  const std::vector<StepOp> p = plan_step(S, nbr, uploads != 0);
+  const std::vector<StepOp> p = plan_steps(S, nbr, steps, uploads != 0);
   if (p.empty()) return fail(SDG_ERR_ARG, "sdg_debug_step_plan: the lists admit no schedule");
   *nops = static_cast<int>(p.size());
   if (4 * *nops > cap)

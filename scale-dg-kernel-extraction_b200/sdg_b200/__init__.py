@@ -86,7 +86,7 @@ SIGNATURES = {
     "sdg_set_kernel_variant": (_I, [_P, _I]),
     "sdg_debug_inject_wait_timeout": (_I, [_P, _I, _I]),
     "sdg_debug_chunk_bounds": (_I, [_I, _I, _I, _P, _I, ctypes.POINTER(_I)]),
-    "sdg_debug_step_plan": (_I, [_I, _P, _P, _I, _P, _I, ctypes.POINTER(_I)]),
+    "sdg_debug_step_plan": (_I, [_I, _P, _P, _I, _I, _P, _I, ctypes.POINTER(_I)]),
     "sdg_minmax_dev_noalloc": (_I, [_P, _LL, _P, _P]),
     "sdg_divlike_dev": (_I, [_I, _I, _LL, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
     "sdg_gradlike_dev": (_I, [_I, _LL, _P, _P, _P, _P, _P, _I, _P]),
@@ -426,18 +426,18 @@ def chunk_bounds(Ne, Np, reach):
     return e0[: n.value + 1] if n.value else e0[:0]
 
 
-def step_plan(nbr, uploads):
-    """Launch order of one chunked RK step over len(nbr) chunks with
-    neighbour lists nbr (host logic): rows (stage, first chunk, last chunk,
-    upload waited for or -1)."""
+def step_plan(nbr, uploads, steps=1):
+    """Launch order of `steps` chunked RK steps over len(nbr) chunks with
+    neighbour lists nbr (host logic): rows (stage 0 .. 3*steps-1, first
+    chunk, last chunk, upload waited for or -1)."""
     S = len(nbr)
     ptr = np.zeros(S + 1, dtype=np.int32)
     ptr[1:] = np.cumsum([len(l) for l in nbr])
     idx = np.array([c for l in nbr for c in l] or [0], dtype=np.int32)
-    ops = np.zeros(4 * 3 * S, dtype=np.int32)
+    ops = np.zeros(4 * 3 * steps * S, dtype=np.int32)
     n = ctypes.c_int(0)
-    _check(lib().sdg_debug_step_plan(S, _p(ptr), _p(idx), int(bool(uploads)), _p(ops),
-                                     ops.size, ctypes.byref(n)))
+    _check(lib().sdg_debug_step_plan(S, _p(ptr), _p(idx), steps, int(bool(uploads)),
+                                     _p(ops), ops.size, ctypes.byref(n)))
     return ops[: 4 * n.value].reshape(-1, 4)
 
 

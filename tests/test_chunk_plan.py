@@ -49,15 +49,15 @@ def test_chunk_bounds(Ne, Np, reach, S):
         assert (size[:3] == thin).all() and (size[-4:] == thin).all()
 
 
-def simulate(plan, nbr, uploads):
-    """Checks every dependency of the plan; returns the chunks whose stage 3
-    runs after the wait for the last upload."""
-    S = len(nbr)
-    done = np.zeros((3, S), dtype=bool)
+def simulate(plan, nbr, uploads, steps=1):
+    """Checks every dependency of the plan; returns the chunks whose last
+    stage runs after the wait for the last upload."""
+    S, G = len(nbr), 3 * steps
+    done = np.zeros((G, S), dtype=bool)
     waited = -1
     late = []
     for g, j0, j1, need in plan:
-        assert 0 <= g <= 2 and 0 <= j0 <= j1 < S
+        assert 0 <= g < G and 0 <= j0 <= j1 < S
         waited = max(waited, need)
         for j in range(j0, j1 + 1):
             assert not done[g, j], "launched twice"
@@ -66,26 +66,29 @@ def simulate(plan, nbr, uploads):
                     assert not uploads or c <= waited, "reads a chunk not yet uploaded"
                 else:
                     assert done[g - 1, c], "reads a stage input not yet written"
-            if g == 2:
-                # q0 of chunk j is overwritten now: every chunk that reads it
-                # in stage 1 (the chunks whose lists hold j) has run.
+            if g >= 2:
+                # Stage g overwrites a buffer (q0 for g % 3 == 2, else the
+                # output of stage g - 3) that stage g - 2 of every chunk
+                # whose list holds j reads: all of them have run.
                 for k in range(S):
                     if j in nbr[k]:
-                        assert done[0, k]
-                if uploads and waited == S - 1:
-                    late.append(j)
+                        assert done[g - 2, k], "overwrites a buffer still to be read"
+            if g == G - 1 and uploads and waited == S - 1:
+                late.append(j)
         done[g, j0:j1 + 1] = True
     assert done.all()
     return late
 
 
-@pytest.mark.parametrize("S", [4, 5, 8, 16, 20])
-def test_step_plan_with_uploads(S):
+@pytest.mark.parametrize("S,steps", [(4, 1), (5, 1), (8, 1), (16, 1), (20, 1),
+                                     (20, 2), (20, 3), (8, 3)])
+def test_step_plan_with_uploads(S, steps):
     nbr = ring(S)
-    plan = sdg.step_plan(nbr, uploads=True)
-    late = simulate(plan, nbr, True)
-    # The last upload's chunk and its neighbours to a depth of three.
-    assert sorted(late) == sorted({j % S for j in range(S - 4, S + 3)})
+    plan = sdg.step_plan(nbr, uploads=True, steps=steps)
+    late = simulate(plan, nbr, True, steps)
+    # The last upload's chunk and its neighbours to a depth of three a step.
+    r = 3 * steps
+    assert sorted(late) == sorted({j % S for j in range(S - 1 - r, S + r)})
     # Stage 0 waits for the uploads in chunk order.
     needs = [n for g, _, _, n in plan if g == 0]
     assert needs == sorted(needs)

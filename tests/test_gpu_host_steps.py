@@ -61,6 +61,8 @@ def pinned_copy(q, mesh):
     ((16, 16, 32), 3, 0, 2),                    # thin end chunks, 16 chunks
     ((16, 16, 32), 2, sdg.FLAG_EXACT, 1),       # the same, exact arithmetic
     ((8, 8, 16), 15, sdg.FLAG_MIXED, 1),        # thin chunks of one z-layer
+    ((16, 16, 16), 3, 0, 3),                    # three steps as one plan
+    ((16, 16, 32), 3, 0, 5),                    # first and last steps by chunks
 ])
 def test_host_steps_equal_three_calls(dims, p, flags, nsteps):
     ops, mesh, fields, dt = make(dims, p, flags)
